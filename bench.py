@@ -1,0 +1,365 @@
+"""Benchmark: Rodas5P ensemble solves/s on the Robertson configuration (one B200).
+
+Workload (the configuration the headline metric is quoted on): Robertson
+chemical kinetics, 3 states, 65,536 trajectories per GPU, rates k1 = 0.04,
+k2 = 3e7, k3 = 1e4 each scaled by log-uniform[0.5, 2], y0 = (1, 0, 0), 20 save
+times on [0, 1e5], rtol 1e-6, atol 1e-10, FP32 LU through the persistent refill
+kernel.  One step = one full ensemble solve.
+
+* ``value``  -- solves/s with inputs resident in HBM, device time (CUDA events on
+  the launching stream), max over ranks; L2 (126 MB) is flushed between steps by
+  writing a 256 MB buffer outside the timed launches.
+* ``e2e``    -- the same through the public ``rodas5P.solve`` call with pinned host
+  inputs: host->device copies, the solve and the device->host read of the
+  history and counters inside the timed region (host wall clock).
+* ``vs_plain`` -- the plain FP64 one-launch kernel (the reference's design) on the
+  same ensemble, device-timed.
+* ``roofline`` -- algorithmic FP64 + LU operations per launch (traced-graph counts
+  x the step counts the kernel reports) against the measured CUDA-core FMA peaks.
+* ``cpu_baseline`` -- the CPU oracle (C++/OpenMP restatement of the reference
+  solver) on a bounded sample, all host cores, rank 0 at N=1 only.
+
+``--impl reference`` times the reference's algorithm on the host instead (the
+oracle port: the reference's own implementation needs numba-cuda-mlir, Enzyme and
+JAX, none of which exist here) and prints the same line with ``"impl": "reference"``.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ensemble solves/s & gradients/s at fixed error vs FP64 oracle, vs plain kernel"
+N_TRAJ = 65536
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_TRAJ)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config_dict(n_total, world):
+    return {
+        "workload": "Robertson Rodas5P, 3 states, FP32 LU, persistent refill kernel",
+        "trajectories_per_gpu": n_total // world,
+        "save_times": 20,
+        "rtol": 1e-6,
+        "atol": 1e-10,
+        "l2": "flushed between timed steps (256 MB write)",
+        "parallelism": f"replicas x{world} (independent trajectory ranges)",
+    }
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.uuid}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        mhz, max_mhz, reasons = [], None, set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                mhz.append(float(parts[0]))
+                max_mhz = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                  "sw_power_cap"), parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(mhz) if mhz else None,
+            "sm_max_mhz": max_mhz,
+            "reasons": sorted(reasons),
+            "samples": len(mhz),
+        }
+
+
+# --------------------------------------------------------------------------- helpers
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_sample_solve(cfg, n_sample, lu_precision):
+    """The oracle on the first ``n_sample`` trajectories, every host thread."""
+    from oracle import oracle
+
+    oracle.build()
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"][:n_sample], cfg["t_span"],
+                 cfg["params"][:n_sample], rtol=cfg["rtol"], atol=cfg["atol"],
+                 lu_precision=lu_precision, threads=threads)
+    dt = time.perf_counter() - t0
+    return n_sample / dt, threads, dt
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from menodax_b200 import systems
+
+    cfg = systems.robertson_config(size=args.n)
+    sample = 8192
+    for _ in range(args.warmup):
+        cpu_sample_solve(cfg, 1024, "fp32")
+    rates, threads, total = [], 0, 0.0
+    for _ in range(args.steps):
+        r, threads, dt = cpu_sample_solve(cfg, sample, "fp32")
+        rates.append(r)
+        total += dt
+    value = sample * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 LU)", "data": "synthetic (seed 42)",
+        "config": config_dict(args.n * world, world),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} of the {args.n} trajectories per step, C++ oracle, OpenMP"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference kernels need numba-cuda-mlir, numba-enzyme and JAX (absent); "
+                "this is the CPU restatement of the same algorithm",
+    }
+    print(json.dumps(line))
+
+
+# --------------------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    from menodax_b200 import _native, rodas5P, systems
+    from menodax_b200._ensemble import launch
+    from menodax_b200._flops import rodas5p_cost
+    from menodax_b200._problem import KernelOptions, get_problem
+
+    rank, world, local = dist_setup(args)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = args.n
+    cfg = systems.robertson_config(size=n, seed=42 + rank)
+    fn = cfg["ode_fn"]
+
+    fp32 = get_problem(fn, 3, 3, KernelOptions(lu_precision="fp32"))
+    fp64 = get_problem(fn, 3, 3, KernelOptions(lu_precision="fp64"))
+    y0 = torch.as_tensor(cfg["y0"], device=dev).contiguous()
+    params = torch.as_tensor(cfg["params"], device=dev).contiguous()
+    times = torch.as_tensor(cfg["t_span"], device=dev).contiguous()
+    hist = torch.empty((n, times.numel(), 3), dtype=torch.float64, device=dev)
+    counters = torch.empty((4, n), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def solve(problem, mode):
+        return launch(problem, y0=y0, times=times, params=params, weights=None, dt0=0.0,
+                      rtol=cfg["rtol"], atol=cfg["atol"], max_steps=100000, mode=mode,
+                      out=(hist, counters))
+
+    def timed(problem, mode, steps, warmup):
+        for _ in range(warmup):
+            solve(problem, mode)
+        barrier(world)
+        evs = []
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solve(problem, mode)
+            e1.record(stream)
+            evs.append((e0, e1))
+        barrier(world)
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return ms
+
+    # warm the modules (load + first launch) outside any timing
+    solve(fp32, _native.MDX_LAUNCH_PERSISTENT)
+    solve(fp64, _native.MDX_LAUNCH_PLAIN)
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid) if uuid else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ms = timed(fp32, _native.MDX_LAUNCH_PERSISTENT, args.steps, args.warmup)
+    clocks = sampler.stop() if sampler else {}
+    total_ms = max_over_ranks(sum(ms), world)
+    value = n * world * args.steps / (total_ms * 1e-3)
+    steps_done = counters[2].to(torch.int64).sum().item()
+    n_saves = n * (times.numel() - 1)
+
+    # the plain FP64 one-launch kernel and the other two variants, same ensemble
+    variants = {}
+    for name, prob, mode in (("plain_fp64", fp64, _native.MDX_LAUNCH_PLAIN),
+                             ("plain_fp32", fp32, _native.MDX_LAUNCH_PLAIN),
+                             ("persistent_fp64", fp64, _native.MDX_LAUNCH_PERSISTENT)):
+        v_ms = timed(prob, mode, max(3, args.steps // 2), 2)
+        t = max_over_ranks(sum(v_ms), world)
+        variants[name] = n * world * len(v_ms) / (t * 1e-3)
+
+    # roofline of the timed kernel
+    cost = rodas5p_cost(fn, 3, 3)
+    peak64 = _native.measure_fma_peak(True)
+    peak32 = _native.measure_fma_peak(False)
+    per_launch_f64 = steps_done * cost.f64 + n_saves * cost.per_save
+    per_launch_f32 = steps_done * cost.lu
+    launch_s = (sum(ms) / len(ms)) * 1e-3
+    t_roof = per_launch_f64 / peak64 + per_launch_f32 / peak32
+    achieved = (per_launch_f64 + per_launch_f32) / launch_s
+    blended_peak = (per_launch_f64 + per_launch_f32) / t_roof
+    traffic_path = ROOT / "profiles" / "robertson_traffic.json"
+    traffic = None
+    if traffic_path.exists():
+        try:
+            traffic = json.loads(traffic_path.read_text()).get("bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+
+    # end to end through the public API, pinned host buffers
+    y0_h = torch.as_tensor(cfg["y0"]).pin_memory()
+    p_h = torch.as_tensor(cfg["params"]).pin_memory()
+    t_h = torch.as_tensor(cfg["t_span"]).pin_memory()
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp32", return_stats=True,
+              launch="persistent")
+    for _ in range(args.warmup):
+        rodas5P.solve(fn, y0_h, t_h, p_h, **kw)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out, st = rodas5P.solve(fn, y0_h, t_h, p_h, **kw)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = n * world * args.steps / e2e_s
+    h2d = y0_h.numel() * 8 + p_h.numel() * 8 + t_h.numel() * 8
+    d2h = out.numel() * 8 + 3 * n * 4
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = 8192
+        rate, threads, _ = cpu_sample_solve(cfg, sample, "fp32")
+        cpu = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"first {sample} of the {n} trajectories, FP32 LU, C++ oracle with OpenMP"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (FP32 LU)", "data": "synthetic (seed 42 + rank)",
+            "config": config_dict(n * world, world),
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "vs_plain": {k: v for k, v in variants.items()},
+            "speedup_vs_plain_fp64": value / variants["plain_fp64"],
+            "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": blended_peak / 1e12,
+                         "unit": "TFLOP/s", "frac": achieved / blended_peak, "traffic": traffic,
+                         "peak_fp64_measured": peak64 / 1e12, "peak_fp32_measured": peak32 / 1e12,
+                         "ops_per_launch_fp64": per_launch_f64, "ops_per_launch_lu_fp32": per_launch_f32,
+                         "attempted_steps_per_launch": steps_done},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/* menodax_b200 C ABI: ensemble ODE integration on one B200 (sm_100a).
+ *
+ * This is the boundary a host framework binds.  It replaces the reference's
+ * device-launch boundary, which is
+ *   - the XLA FFI handler `modax_numba_cuda_abi_launch`
+ *     (modax/_jax_numba_custom_call.py:145-231): buffers + attrs -> cuLaunchKernel
+ *     of a numba-compiled cubin on XLA's stream, errors as ffi::Error;
+ *   - its Python callers `ensemble_ffi_call` / `ffi_abi_call`
+ *     (modax/_numba_common.py:84-130, modax/_jax_numba_custom_call.py:333-371),
+ *     which fix the argument order y0, times, params, dt0, rtol, atol, max_steps,
+ *     weights -> hist, accepted, rejected, loop_steps (modax/_numba_common.py:27-40);
+ *   - cubin loading and function lookup `compile_kernel`
+ *     (modax/_jax_numba_custom_call.py:286-314).
+ *
+ * Conventions: plain C types only; every call returns an int status (MDX_OK or a
+ * negative MDX_E_* code) and never aborts or traps; mdx_last_error() gives the
+ * calling thread's last message.  Device buffers are owned by the caller; a plan
+ * owns its compiled modules.  Arrays are row-major, the trajectory index slowest.
+ * `stream` is a CUstream / cudaStream_t (NULL = legacy default stream).
+ */
+#ifndef MENODAX_H
+#define MENODAX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDX_ABI_VERSION 1
+
+#define MDX_OK 0
+#define MDX_E_INVALID (-1)     /* bad argument (ffi::ErrorCode::kInvalidArgument) */
+#define MDX_E_COMPILE (-2)     /* NVRTC rejected the source */
+#define MDX_E_CUDA (-3)        /* a CUDA driver call failed (ffi::ErrorCode::kInternal) */
+#define MDX_E_NO_DRIVER (-4)   /* libcuda.so.1 could not be loaded */
+#define MDX_E_NOMEM (-5)
+
+#define MDX_SOLVER_TSIT5 1
+#define MDX_SOLVER_RODAS5P 2
+
+#define MDX_LAUNCH_PLAIN 0      /* one trajectory per thread, grid = ceil(N / tpb) */
+#define MDX_LAUNCH_PERSISTENT 1 /* device-sized grid, warps refill from a queue */
+
+#define MDX_PLAN_CHECKPOINT 1   /* the module records accepted step states */
+#define MDX_PLAN_ADJOINT 2      /* the module carries the discrete-adjoint kernel */
+
+/* Per-trajectory status bits written to mdx_solve_desc.status. */
+#define MDX_STATUS_OK 0
+#define MDX_STATUS_MAX_STEPS 1
+#define MDX_STATUS_NONFINITE 2
+#define MDX_STATUS_CKPT_OVERFLOW 4
+
+typedef struct mdx_plan mdx_plan;
+
+/* A compiled problem.  `cubin` is the output of mdx_compile for the source the
+ * Python host generates from a traced right-hand side; it is copied.  Replaces
+ * the cubin + CUfunction pair modax keeps per kernel (compile_kernel,
+ * modax/_jax_numba_custom_call.py:286-314). */
+typedef struct mdx_plan_desc {
+  int struct_size;        /* sizeof(mdx_plan_desc) */
+  int solver;             /* MDX_SOLVER_* */
+  int n_vars;             /* state components of the base system */
+  int n_system;           /* integrated components (n_vars * (1 + n_sens)) */
+  int n_params;
+  int threads_per_block;  /* the block size the module was compiled for */
+  int flags;              /* MDX_PLAN_* */
+  int reserved;
+  const void* cubin;
+  size_t cubin_size;
+} mdx_plan_desc;
+
+/* One ensemble solve: the reference's SOLVER_ARGTYPES plus a status array, an
+ * optional persistent-kernel workspace and optional checkpoint buffers. */
+typedef struct mdx_solve_desc {
+  int struct_size;        /* sizeof(mdx_solve_desc) */
+  int mode;               /* MDX_LAUNCH_* */
+  int n_traj;
+  int n_save;             /* len(times) */
+  int n_save_hist;        /* rows of hist per trajectory: n_save, or 1 without history */
+  int max_steps;
+  double dt0;             /* <= 0: 1e-6 of the integration window */
+  double rtol;
+  double atol;
+  const double* y0;       /* (n_traj, n_system) */
+  const double* times;    /* (n_save,) */
+  const double* params;   /* (n_traj, n_params) */
+  const double* weights;  /* (n_traj, n_system), or NULL for constant weights */
+  double* hist;           /* (n_traj, n_save_hist, n_system) */
+  int* accepted;          /* (n_traj,) */
+  int* rejected;          /* (n_traj,) */
+  int* loop_steps;        /* (n_traj,) */
+  int* status;            /* (n_traj,) or NULL */
+  double* hook_out;       /* reserved, NULL */
+  const int* order;       /* persistent: optional trajectory visiting order, or NULL */
+  void* workspace;        /* persistent: >= mdx_workspace_size() bytes */
+  size_t workspace_bytes;
+  double* ckpt;           /* MDX_PLAN_CHECKPOINT: (ckpt_capacity, n_traj, n_vars + 2) */
+  int* ckpt_count;        /* MDX_PLAN_CHECKPOINT: (n_traj,) */
+  long long ckpt_capacity;
+  int grid_blocks;        /* persistent: 0 = occupancy-sized */
+  int reserved;
+} mdx_solve_desc;
+
+/* The reverse pass of the discrete adjoint over checkpoints a MDX_PLAN_CHECKPOINT
+ * solve recorded.  No counterpart in the reference, whose gradients come from
+ * forward sensitivities (modax/_sensitivity.py:331-413); this is the backward of
+ * the torch.autograd.Function / jax.custom_vjp front ends. */
+typedef struct mdx_grad_desc {
+  int struct_size;        /* sizeof(mdx_grad_desc) */
+  int n_traj;
+  int n_save;
+  int reserved;
+  const double* times;
+  const double* params;
+  const double* ckpt;
+  const int* ckpt_count;
+  long long ckpt_capacity;
+  const double* grad_hist; /* (n_traj, n_save, n_vars) */
+  double* grad_y0;         /* (n_traj, n_vars), overwritten */
+  double* grad_params;     /* (n_traj, n_params), overwritten */
+  int* status;             /* (n_traj,) or NULL */
+} mdx_grad_desc;
+
+/* NVRTC: compile CUDA C++ `source` to an sm_100a cubin.  Needs no GPU.
+ * On success *cubin is malloc'd (release with mdx_free).  `log` (may be NULL)
+ * receives the compiler log, truncated to log_size. */
+int mdx_compile(const char* source, const char* program_name, const char* const* options,
+                int n_options, void** cubin, size_t* cubin_size, char* log, size_t log_size);
+void mdx_free(void* ptr);
+
+int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan);
+int mdx_plan_destroy(mdx_plan* plan);
+
+/* Bytes of `workspace` a solve in `mode` needs (0 for MDX_LAUNCH_PLAIN). */
+int mdx_workspace_size(const mdx_plan* plan, int mode, int n_traj, size_t* bytes);
+
+/* Resident blocks per SM for the plan's kernel in `mode`, and the SM count of
+ * the current device (loads the module on first use). */
+int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count);
+
+/* Launch one ensemble solve on `stream`.  Asynchronous. */
+int mdx_solve(mdx_plan* plan, const mdx_solve_desc* desc, void* stream);
+
+/* Launch the discrete-adjoint reverse pass on `stream` (MDX_PLAN_ADJOINT plans). */
+int mdx_grad(mdx_plan* plan, const mdx_grad_desc* desc, void* stream);
+
+/* Measured FMA throughput of the current device's CUDA cores, in FLOP/s
+ * (an FMA counts two): the roofline denominator of the ensemble kernels, which
+ * are bound by FP64/FP32 issue rather than HBM or the tensor cores.  No
+ * counterpart in the reference. */
+int mdx_measure_fma_peak(int double_precision, double* flops_per_s);
+
+/* The calling thread's last error message. Returns its full length. */
+int mdx_last_error(char* buf, size_t buf_size);
+
+const char* mdx_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

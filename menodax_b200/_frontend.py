@@ -1,0 +1,100 @@
+"""The common body of ``tsit5.solve`` and ``rodas5P.solve``.
+
+Inputs may be NumPy arrays (results come back as NumPy, like the reference's
+host-array calls) or torch tensors (results stay on their CUDA device; CPU
+tensors are copied in and the results copied back).  A torch input that
+requires grad routes through the discrete adjoint (``menodax_b200.autograd``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from menodax_b200 import _native
+from menodax_b200._ensemble import (
+    build_error_weights,
+    initial_step,
+    launch,
+    normalize_y0_params,
+    pick_device,
+    solver_stats,
+    to_device,
+)
+from menodax_b200._problem import KernelOptions, get_problem
+
+LAUNCH_MODES = ("auto", "plain", "persistent")
+
+
+def _is_torch(*xs):
+    return any(isinstance(x, torch.Tensor) for x in xs)
+
+
+def _times_tensor(t_span):
+    if isinstance(t_span, torch.Tensor):
+        t = t_span.detach().to(torch.float64)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(np.asarray(t_span, dtype=np.float64)))
+    if t.ndim != 1 or t.shape[0] < 1:
+        raise ValueError(f"t_span must be a 1-D array of save times; got shape {tuple(t.shape)}")
+    return t
+
+
+def resolve_mode(launch_mode: str, options: KernelOptions, n: int) -> int:
+    if launch_mode not in LAUNCH_MODES:
+        raise ValueError(f"launch must be one of {LAUNCH_MODES}; got {launch_mode!r}")
+    if launch_mode == "plain":
+        return _native.MDX_LAUNCH_PLAIN
+    if launch_mode == "persistent":
+        return _native.MDX_LAUNCH_PERSISTENT
+    # Uneven step counts are what the refill kernel is for; a stiff solve whose
+    # ensemble fills more than one wave of warps gains from it.
+    if options.solver == "rodas5P" and n >= 4096:
+        return _native.MDX_LAUNCH_PERSISTENT
+    return _native.MDX_LAUNCH_PLAIN
+
+
+def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first_step,
+        max_steps, return_stats, error_weights, launch_mode="auto", grid_blocks=0):
+    torch_io = _is_torch(y0, params)
+    y0_t, p_t, n, n_vars = normalize_y0_params(y0, params)
+    n_params = p_t.shape[1]
+    times = _times_tensor(t_span)
+    weights = build_error_weights(error_weights, n, n_vars)
+    if weights is not None:
+        options = _replace(options, runtime_weights=True)
+    if options.tf_index >= 0 and not options.tf_index < n_params:
+        raise ValueError(f"tf_index {options.tf_index} is outside the {n_params} parameter columns")
+    if int(max_steps) < 0:
+        raise ValueError("max_steps must be non-negative")
+    device = pick_device(y0_t, p_t)
+    problem = get_problem(ode_fn, n_vars, n_params, options)
+    mode = resolve_mode(launch_mode, options, n)
+    y0_d = to_device(y0_t.detach(), device)
+    p_d = to_device(p_t.detach(), device)
+    t_d = to_device(times, device)
+    w_d = to_device(weights.detach(), device) if weights is not None else None
+    hist, acc, rej, loop, status = launch(
+        problem, y0=y0_d, times=t_d, params=p_d, weights=w_d, dt0=initial_step(first_step),
+        rtol=rtol, atol=atol, max_steps=max_steps, mode=mode,
+        n_save_hist=None if options.save_history else 1, grid_blocks=grid_blocks,
+    )
+    input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
+    if torch_io and input_on_gpu:
+        out = (hist,)
+        stats = solver_stats(acc, rej, loop)
+    elif torch_io:
+        out = (hist.cpu(),)
+        stats = solver_stats(acc.cpu(), rej.cpu(), loop.cpu())
+    else:
+        out = (hist.cpu().numpy(),)
+        stats = solver_stats(acc.cpu().numpy(), rej.cpu().numpy(), loop.cpu().numpy())
+    if return_stats:
+        return out[0], stats
+    return out[0]
+
+
+def _replace(options, **kw):
+    from dataclasses import replace
+
+    return replace(options, **kw)

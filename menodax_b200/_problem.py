@@ -1,0 +1,214 @@
+"""Build the NVRTC source of one problem, compile it, and cache the plan.
+
+This is the host-side planning layer of the reference (``KernelOptions`` and
+``_make_kernel``, ``modax/rodas5P.py:137-165, 306-1007``; ``modax/tsit5.py:156-487``):
+everything that selects a compiled kernel besides the right-hand side and the
+shapes is a field of ``KernelOptions``, which is also the cache key.
+"""
+
+from __future__ import annotations
+
+import threading
+from dataclasses import dataclass
+
+from menodax_b200 import _native
+from menodax_b200._codegen import (
+    SensLayout,
+    emit_adjoint_pieces,
+    emit_neg_jac,
+    emit_rhs,
+    emit_sens_coupling,
+    lit,
+)
+from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
+from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparsity import dense_jacobian
+from menodax_b200._trace import trace
+
+TSIT5_EXPONENT = -1.0 / 5.0   # modax/tsit5.py:90
+RODAS5P_EXPONENT = -1.0 / 6.0  # modax/rodas5P.py:113
+
+
+@dataclass(frozen=True)
+class KernelOptions:
+    """Everything besides ``ode_fn`` and the sizes that selects a compiled kernel."""
+
+    solver: str = "rodas5P"
+    pcoeff: float = 0.0
+    icoeff: float = 1.0
+    dcoeff: float = 0.0
+    lu_precision: str = "fp32"
+    threads_per_block: int = 32
+    min_blocks: int = 1
+    sparsity: tuple | None = None
+    ordering: str = "amd"
+    tf_index: int = -1
+    max_registers: int | None = None
+    save_history: bool = True
+    runtime_weights: bool = False
+    # Forward sensitivities: (n_y0_dirs, param columns, error_control), or None.
+    sens: tuple | None = None
+    checkpoint: bool = False
+    adjoint: bool = False
+
+
+def controller_exponents(options: KernelOptions):
+    exponent = TSIT5_EXPONENT if options.solver == "tsit5" else RODAS5P_EXPONENT
+    e1 = exponent * (options.icoeff + options.pcoeff + options.dcoeff)
+    e2 = -exponent * (options.pcoeff + 2.0 * options.dcoeff)
+    e3 = exponent * options.dcoeff
+    return e1, e2, e3
+
+
+@dataclass
+class Problem:
+    """A compiled problem: its plan plus what the host needs to call it."""
+
+    plan: _native.Plan
+    source: str
+    n_vars: int
+    n_system: int
+    n_params: int
+    n_error: int
+    options: KernelOptions
+    lu_size: int
+    sparse: object = None
+
+
+def _sens_layout(n_vars, n_params, sens):
+    if sens is None:
+        return None
+    n_y0_dirs, cols, _ = sens
+    return SensLayout(n_vars, n_params, n_y0_dirs, tuple(cols))
+
+
+def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
+    """Generate the full NVRTC source; returns ``(source, meta)``."""
+    tr = trace(ode_fn, n_vars, n_params)
+    sens = _sens_layout(n_vars, n_params, options.sens)
+    n_sens = 0 if sens is None else sens.n_sens
+    n_system = n_vars * (1 + n_sens)
+    error_control = True if options.sens is None else bool(options.sens[2])
+    n_error = n_system if error_control else n_vars
+    e1, e2, e3 = controller_exponents(options)
+    rodas = options.solver == "rodas5P"
+    lu_t = "float" if options.lu_precision == "fp32" else "double"
+    parts = [
+        f"// generated problem source: {options.solver}, n_vars={n_vars}, n_params={n_params}, n_sens={n_sens}",
+        f"#define MDX_NV {n_vars}",
+        f"#define MDX_NS {n_system}",
+        f"#define MDX_NP {n_params}",
+        f"#define MDX_NSENS {n_sens}",
+        f"#define MDX_NERR {lit(float(n_error))}",
+        f"#define MDX_LU_T {lu_t}",
+        f"#define MDX_TF_INDEX {int(options.tf_index)}",
+        f"#define MDX_E1 {lit(e1)}",
+        f"#define MDX_E2 {lit(e2)}",
+        f"#define MDX_E3 {lit(e3)}",
+        f"#define MDX_USE_E2 {'true' if e2 != 0.0 else 'false'}",
+        f"#define MDX_USE_E3 {'true' if e3 != 0.0 else 'false'}",
+        f"#define MDX_WEIGHTS_RUNTIME {1 if options.runtime_weights else 0}",
+        f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
+        f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
+        f"#define MDX_TPB {int(options.threads_per_block)}",
+        f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
+        '#include "mdx_common.cuh"',
+    ]
+    sens_weight = "1.0" if error_control else "0.0"
+    parts.append(
+        "__device__ __forceinline__ double mdx_const_weight(int j) "
+        f"{{ return j < MDX_NV ? 1.0 : {sens_weight}; }}"
+    )
+    parts.append(emit_rhs(tr, sens))
+    lu_size = 0
+    sparse = None
+    if rodas:
+        if options.sparsity is None:
+            structure = dense_jacobian(n_vars)
+            lu_size = n_vars * n_vars
+            parts.append(f"#define MDX_LU_SIZE {lu_size}")
+            parts.append(f"#define MDX_IPIV {n_vars}")
+            parts.append('#include "mdx_dense_lu.cuh"')
+            parts.append(
+                "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP& ipiv) "
+                "{ mdx::dense_factorize<MDX_NV, MDX_LU_T>(lu, ipiv); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP& ipiv, R& rhs) "
+                "{ mdx::dense_solve<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP& ipiv, R& rhs) "
+                "{ mdx::dense_solve_t<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "__device__ __forceinline__ int mdx_diag_slot(int d) { return d * MDX_NV + d; }"
+            )
+        else:
+            sparse = sparse_direct_solver_for(options.sparsity, options.ordering)
+            structure = sparse.compressed
+            lu_size = structure.size
+            parts.append(f"#define MDX_LU_SIZE {lu_size}")
+            parts.append("#define MDX_IPIV 1")
+            parts.append(emit_sparse_lu(sparse.layout, sparse.ops))
+            diag = structure.diagonal
+            cases = " ".join(f"case {d}: return {int(s)};" for d, s in enumerate(diag))
+            parts.append(
+                "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP&) "
+                "{ mdx_sparse_factorize<MDX_LU_T>(lu); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP&, R& rhs) "
+                "{ mdx_sparse_solve<MDX_LU_T>(lu, rhs); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP&, R& rhs) "
+                "{ mdx_sparse_solve_t<MDX_LU_T>(lu, rhs); }\n"
+                f"__device__ __forceinline__ int mdx_diag_slot(int d) {{ switch (d) {{ {cases} default: return 0; }} }}"
+            )
+        parts.append(emit_neg_jac(tr, structure, lu_size, sens))
+        if sens is not None:
+            parts.append(emit_sens_coupling(tr, sens))
+        parts.append('#include "mdx_rodas5p.cuh"')
+        parts.append("#define MDX_SOLVER mdx::Rodas5P")
+    else:
+        parts.append("#define MDX_LU_SIZE 1")
+        parts.append('#include "mdx_tsit5.cuh"')
+        parts.append("#define MDX_SOLVER mdx::Tsit5")
+    parts.append('#include "mdx_entry.cuh"')
+    if options.adjoint:
+        parts.append(emit_adjoint_pieces(tr))
+        parts.append('#include "mdx_adjoint.cuh"')
+    meta = dict(n_system=n_system, n_error=n_error, lu_size=lu_size, sparse=sparse)
+    return "\n".join(parts) + "\n", meta
+
+
+def compile_options(options: KernelOptions) -> list[str]:
+    opts = []
+    if options.max_registers is not None:
+        opts.append(f"--maxrregcount={int(options.max_registers)}")
+    return opts
+
+
+_cache: dict = {}
+_cache_lock = threading.Lock()
+
+
+def get_problem(ode_fn, n_vars: int, n_params: int, options: KernelOptions) -> Problem:
+    """The compiled problem for these options, built once per process."""
+    key = (ode_fn, n_vars, n_params, options)
+    with _cache_lock:
+        found = _cache.get(key)
+    if found is not None:
+        return found
+    source, meta = build_source(ode_fn, n_vars, n_params, options)
+    cubin = _native.compile_cubin(source, compile_options(options))
+    flags = (_native.MDX_PLAN_CHECKPOINT if options.checkpoint else 0) | (
+        _native.MDX_PLAN_ADJOINT if options.adjoint else 0
+    )
+    solver = _native.MDX_SOLVER_TSIT5 if options.solver == "tsit5" else _native.MDX_SOLVER_RODAS5P
+    plan = _native.Plan(solver, n_vars, meta["n_system"], n_params, options.threads_per_block, flags, cubin)
+    prob = Problem(
+        plan=plan, source=source, n_vars=n_vars, n_system=meta["n_system"], n_params=n_params,
+        n_error=meta["n_error"], options=options, lu_size=meta["lu_size"], sparse=meta["sparse"],
+    )
+    with _cache_lock:
+        _cache.setdefault(key, prob)
+        return _cache[key]
+
+
+def clear_caches() -> None:
+    """Drop every compiled problem (``modax/tsit5.py:142-153``)."""
+    with _cache_lock:
+        _cache.clear()
+    sparse_direct_solver_for.cache_clear()

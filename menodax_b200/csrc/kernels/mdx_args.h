@@ -1,0 +1,58 @@
+/* Kernel parameter blocks, identical in layout on the host (C++ runtime) and on
+ * the device (NVRTC-compiled kernels).  Plain C with fixed-width-free types so the
+ * header compiles under NVRTC, which has no standard library headers.
+ *
+ * Array layouts follow the reference's FFI call (modax/_numba_common.py:24-42):
+ * y0 (N, n_system), times (S,), params (N, n_params), weights (N, n_system),
+ * hist (N, S_hist, n_system), and three (N,) int32 counters; all row-major.
+ */
+#ifndef MDX_ARGS_H
+#define MDX_ARGS_H
+
+/* Per-trajectory status written by every solve kernel. */
+#define MDX_STATUS_OK 0
+#define MDX_STATUS_MAX_STEPS 1     /* max_steps reached before the last save time */
+#define MDX_STATUS_NONFINITE 2     /* the final state holds a NaN or an infinity */
+#define MDX_STATUS_CKPT_OVERFLOW 4 /* more accepted steps than checkpoint capacity */
+
+typedef struct MdxSolveArgs {
+  const double* y0;
+  const double* times;
+  const double* params;
+  const double* weights;   /* may be NULL when the kernel was built with constant weights */
+  double* hist;
+  int* accepted;
+  int* rejected;
+  int* loop_steps;
+  int* status;             /* may be NULL */
+  double* hook_out;        /* (N, hook_size) or NULL */
+  int* work_counter;       /* persistent kernels: queue head, zeroed before launch */
+  const int* order;        /* persistent kernels: optional visiting order (N,) */
+  double* ckpt;            /* adjoint forward pass: (capacity, N, n_vars + 2) step states */
+  int* ckpt_count;         /* adjoint forward pass: accepted steps recorded per trajectory */
+  long long ckpt_capacity; /* steps per trajectory the checkpoint buffer holds */
+  int n_traj;
+  int n_save;
+  int n_save_hist;         /* S, or 1 when only the final state is kept */
+  int max_steps;
+  double dt0;
+  double rtol;
+  double atol;
+} MdxSolveArgs;
+
+typedef struct MdxGradArgs {
+  const double* times;
+  const double* params;
+  const double* ckpt;      /* as written by the forward pass */
+  const int* ckpt_count;
+  const double* grad_hist; /* (N, S, n_vars) cotangent of the history */
+  double* grad_y0;         /* (N, n_vars) */
+  double* grad_params;     /* (N, n_params) */
+  int* status;             /* may be NULL */
+  long long ckpt_capacity;
+  int n_traj;
+  int n_save;
+  int pad;
+} MdxGradArgs;
+
+#endif

@@ -1,0 +1,58 @@
+// Shared device helpers for the ensemble ODE kernels (sm_100a, NVRTC-compiled).
+//
+// Every kernel runs one trajectory per thread.  A problem header generated on
+// the host (menodax_b200/_codegen.py) defines the sizes, the traced right-hand
+// side and its derivatives as force-inlined templates; with every component
+// index a compile-time constant the per-trajectory vectors live in registers.
+#pragma once
+#include "mdx_args.h"
+
+#define MDX_FULL_MASK 0xffffffffu
+
+#ifndef MDX_TPB
+#define MDX_TPB 32
+#endif
+#ifndef MDX_MIN_BLOCKS
+#define MDX_MIN_BLOCKS 1
+#endif
+
+namespace mdx {
+
+// Python's max(a, b) on floats: the first argument unless the second is larger.
+// It differs from fmax only on NaN, where the reference's comparison semantics
+// (modax/rodas5P.py:907, modax/tsit5.py:297) are kept.
+__device__ __forceinline__ double pymax(double a, double b) { return b > a ? b : a; }
+
+__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
+
+__device__ __forceinline__ double nan_value() { return __longlong_as_double(0x7ff8000000000000LL); }
+
+// Step-size controller (modax/rodas5P.py:913-928, modax/tsit5.py:383-398):
+// clamp the error into [1e-18, 1e18] (NaN counts as huge), form the PID factor
+// from the error history, and clamp the factor.  E2 and E3 are compile-time
+// constants, so the default I-controller multiplies by nothing extra.
+__device__ __forceinline__ double controller_factor(double err_norm, double err_prev,
+                                                    double err_prev2, double e1, double e2,
+                                                    double e3, bool use_e2, bool use_e3,
+                                                    double& safe_err) {
+  if (isnan(err_norm) || err_norm > 1e18) {
+    safe_err = 1e18;
+  } else if (err_norm == 0.0) {
+    safe_err = 1e-18;
+  } else {
+    safe_err = err_norm;
+  }
+  double factor = 0.9 * pow(safe_err, e1);
+  if (use_e2) factor = factor * pow(err_prev, e2);
+  if (use_e3) factor = factor * pow(err_prev2, e3);
+  return factor;
+}
+
+// True when save time `ts` is reached by a step ending at `t_new`
+// (modax/rodas5P.py:933-935): the 1e-12 relative slack keeps a save that
+// rounding puts a hair past the end of the step from being missed.
+__device__ __forceinline__ bool save_reached(double ts, double t_new) {
+  return ts <= t_new + 1e-12 * pymax(1.0, fabs(ts));
+}
+
+}  // namespace mdx

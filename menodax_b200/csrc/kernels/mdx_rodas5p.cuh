@@ -1,0 +1,363 @@
+// Rodas5P (Rosenbrock-W, order 5), one trajectory per thread.
+//
+// Restates the reference kernel's step (modax/rodas5P.py:761-1005) as a
+// state/step/finish triple so the same step body serves the one-launch kernel
+// (one trajectory per thread for its whole life) and the persistent refill
+// kernel (mdx_persistent.cuh), where a lane that finishes takes the next
+// trajectory off a queue.
+//
+// Per step: -J and df/dt from the traced right-hand side (one forward sweep per
+// colour, plus one in t), M = I/(h*gamma) - J on the diagonal slots, one LU, and
+// eight stages "f -> stage right-hand side -> solve" against it; the error
+// estimate is the eighth stage; PID control; dense output on accept.
+//
+// Precision split (modax/rodas5P.py:347-349, 713, 724): the state, f, J, the
+// stage combinations, the error and the controller are double; the matrix, the
+// solver's right-hand side and the stored stage increments k are MDX_LU_T.
+//
+// The problem header included before this file defines the sizes and the
+// traced functions mdx_rhs / mdx_neg_jac / mdx_factorize / mdx_solve (and, with
+// forward sensitivities, mdx_sens_coupling).
+#pragma once
+#include "mdx_common.cuh"
+
+namespace mdx {
+namespace rodas5p {
+
+// W-transformed Rodas5P coefficients (Steinebach 2023, BIT 63:27), as tabulated
+// in modax/rodas5P.py:44-105.  Stages 6-8 accumulate into u (FSAL form), so only
+// five rows of A exist.
+constexpr double GAMMA = 0.21193756319429014;
+__host__ __device__ constexpr double coef_a(int s, int m) {
+  constexpr double t[5][5] = {
+    {3.0, 0, 0, 0, 0},
+    {2.849394379747939, 0.45842242204463923, 0, 0, 0},
+    {-6.954028509809101, 2.489845061869568, -10.358996098473584, 0, 0},
+    {2.8029986275628964, 0.5072464736228206, -0.3988312541770524, -0.04721187230404641, 0},
+    {-7.502846399306121, 2.561846144803919, -11.627539656261098, -0.18268767659942256,
+     0.030198172008377946},
+};
+  return t[s][m];
+}
+__host__ __device__ constexpr double coef_c(int s, int m) {
+  constexpr double t[8][7] = {
+    {0, 0, 0, 0, 0, 0, 0},
+    {-14.155112264123755, 0, 0, 0, 0, 0, 0},
+    {-17.97296035885952, -2.859693295451294, 0, 0, 0, 0, 0},
+    {147.12150275711716, -1.41221402718213, 71.68940251302358, 0, 0, 0, 0},
+    {165.43517024871676, -0.4592823456491126, 42.90938336958603, -5.961986721573306, 0, 0, 0},
+    {24.854864614690072, -3.0009227002832186, 47.4931110020768, 5.5814197821558125,
+     -0.6610691825249471, 0, 0},
+    {30.91273214028599, -3.1208243349937974, 77.79954646070892, 34.28646028294783,
+     -19.097331116725623, -28.087943162872662, 0},
+    {37.80277123390563, -3.2571969029072276, 112.26918849496327, 66.9347231244047,
+     -40.06618937091002, -54.66780262877968, -9.48861652309627},
+};
+  return t[s][m];
+}
+// Stage abscissae of stages 2..5; stage 1 sits at t, stages 6..8 at t + h.
+__host__ __device__ constexpr double coef_ct(int s) {
+  constexpr double t[4] = {0.6358126895828704, 0.4095798393397535, 0.9769306725060716,
+                          0.4288403609558664};
+  return t[s];
+}
+// df/dt coefficients d_i (zero for stages 6..8).
+__host__ __device__ constexpr double coef_d(int s) {
+  constexpr double t[8] = {GAMMA, -0.42387512638858027, -0.3384627126235924, 1.8046452872882734,
+                         2.325825639765069, 0.0, 0.0, 0.0};
+  return t[s];
+}
+// Continuous extension: h1..h3 as combinations of k1..k8 (modax/rodas5P.py:939-968).
+__host__ __device__ constexpr double coef_h(int r, int m) {
+  constexpr double t[3][8] = {
+    {25.948786856663858, -2.5579724845846235, 10.433815404888879, -2.3679251022685204,
+     0.524948541321073, 1.1241088310450404, 0.4272876194431874, -0.17202221070155493},
+    {-9.91568850695171, -0.9689944594115154, 3.0438037242978453, -24.495224566215796,
+     20.176138334709044, 15.98066361424651, -6.789040303419874, -6.710236069923372},
+    {11.419903575922262, 2.8879645146136994, 72.92137995996029, 80.12511834622643,
+     -52.072871366152654, -59.78993625266729, -0.15582684282751913, 4.883087185713722},
+};
+  return t[r][m];
+}
+constexpr double FACTOR_MIN = 0.2;
+constexpr double FACTOR_MAX = 6.0;
+
+typedef MDX_LU_T lu_t;
+
+struct State {
+  double y[MDX_NS];
+  double p[MDX_NP > 0 ? MDX_NP : 1];
+  double t, dt, err_prev, err_prev2, tf_local;
+  int save_idx, n_steps, accepted, rejected, traj;
+#if MDX_CHECKPOINT
+  int n_ckpt;
+  bool ckpt_overflow;
+#endif
+};
+
+__device__ __forceinline__ size_t hist_index(const MdxSolveArgs& a, int traj, int s, int j) {
+  return ((size_t)traj * (size_t)a.n_save_hist + (size_t)s) * (size_t)MDX_NS + (size_t)j;
+}
+
+__device__ __forceinline__ double weight(const MdxSolveArgs& a, int traj, int j) {
+#if MDX_WEIGHTS_RUNTIME
+  return a.weights[(size_t)traj * MDX_NS + j];
+#else
+  return mdx_const_weight(j);
+#endif
+}
+
+__device__ __forceinline__ void init(State& st, const MdxSolveArgs& a, int traj) {
+  st.traj = traj;
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) st.y[j] = a.y0[(size_t)traj * MDX_NS + j];
+#if MDX_SAVE_HISTORY
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) a.hist[hist_index(a, traj, 0, j)] = st.y[j];
+#endif
+#pragma unroll
+  for (int k = 0; k < MDX_NP; ++k) st.p[k] = a.params[(size_t)traj * MDX_NP + k];
+  const double t0 = a.times[0];
+  const double tf = a.times[a.n_save - 1];
+  st.t = t0;
+  st.dt = a.dt0 > 0.0 ? a.dt0 : (tf - t0) * 1e-6;
+  st.save_idx = 1;
+  st.n_steps = 0;
+  st.accepted = 0;
+  st.rejected = 0;
+  st.err_prev = 1.0;
+  st.err_prev2 = 1.0;
+#if MDX_TF_INDEX >= 0
+  st.tf_local = st.p[MDX_TF_INDEX];
+#else
+  st.tf_local = tf;
+#endif
+#if MDX_CHECKPOINT
+  st.n_ckpt = 0;
+  st.ckpt_overflow = false;
+#endif
+}
+
+__device__ __forceinline__ bool running(const State& st, const MdxSolveArgs& a) {
+  return st.save_idx < a.n_save && st.t < st.tf_local && st.n_steps < a.max_steps;
+}
+
+// One Rosenbrock stage: its right-hand side from the tableau row, then the
+// solve against the step's factorisation.  State rows go to the solver's
+// buffer; with forward sensitivities the sensitivity rows wait in `work` until
+// the coupling term L_k k_y of their block is known (modax/rodas5P.py:513-583).
+template <int S, class LU, class IP, class K, class W, class DT, class RB>
+__device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& k, W& work,
+                                      const DT& dT, const State& st, double dt_use,
+                                      double inv_dt) {
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) {
+    double value;
+    if constexpr (S == 0) {
+      value = work[j] + dt_use * coef_d(0) * dT[j];
+    } else {
+      double acc = coef_c(S, 0) * (double)k[0][j];
+#pragma unroll
+      for (int m = 1; m < S; ++m) acc += coef_c(S, m) * (double)k[m][j];
+      if constexpr (coef_d(S) != 0.0) {
+        value = work[j] + dt_use * coef_d(S) * dT[j] + acc * inv_dt;
+      } else {
+        value = work[j] + acc * inv_dt;
+      }
+    }
+    if (j < MDX_NV) rhs[j] = (lu_t)value;
+    else work[j] = value;
+  }
+  mdx_solve(lu, ipiv, rhs);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) k[S][j] = rhs[j];
+#if MDX_NSENS > 0
+  double kstate[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) kstate[j] = (double)k[S][j];
+  double coupling[MDX_NSENS * MDX_NV];
+  mdx_sens_coupling(st.y, st.t, st.p, kstate, coupling);
+#pragma unroll
+  for (int s = 0; s < MDX_NSENS; ++s) {
+    const int base = MDX_NV + s * MDX_NV;
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) rhs[j] = (lu_t)(work[base + j] + coupling[s * MDX_NV + j]);
+    mdx_solve(lu, ipiv, rhs);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) k[S][base + j] = rhs[j];
+  }
+#endif
+}
+
+template <int S, class U, class K>
+__device__ __forceinline__ void advance(U& u, const State& st, const K& k) {
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) {
+    double acc = coef_a(S, 0) * (double)k[0][j];
+#pragma unroll
+    for (int m = 1; m <= S; ++m) acc += coef_a(S, m) * (double)k[m][j];
+    u[j] = st.y[j] + acc;
+  }
+}
+
+__device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
+  double dt_use = st.dt;
+  if (dt_use > st.tf_local - st.t) dt_use = st.tf_local - st.t;
+  if (dt_use < 1e-30) dt_use = 1e-30;
+  const double inv_dt = 1.0 / dt_use;
+  const double t = st.t;
+  const double t_end = t + dt_use;
+  const double dtgamma_inv = 1.0 / (dt_use * GAMMA);
+
+  lu_t lu[MDX_LU_SIZE];
+  int ipiv[MDX_IPIV];
+  double dT[MDX_NS];
+  mdx_neg_jac(st.y, t, st.p, lu, dT);
+#pragma unroll
+  for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (lu_t)dtgamma_inv;
+  mdx_factorize(lu, ipiv);
+
+  lu_t rhs[MDX_NV];
+  lu_t k[8][MDX_NS];
+  double u[MDX_NS];
+  double work[MDX_NS];
+
+  mdx_rhs(st.y, t, st.p, work);
+  stage<0>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  advance<0>(u, st, k);
+  mdx_rhs(u, t + coef_ct(0) * dt_use, st.p, work);
+  stage<1>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  advance<1>(u, st, k);
+  mdx_rhs(u, t + coef_ct(1) * dt_use, st.p, work);
+  stage<2>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  advance<2>(u, st, k);
+  mdx_rhs(u, t + coef_ct(2) * dt_use, st.p, work);
+  stage<3>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  advance<3>(u, st, k);
+  mdx_rhs(u, t + coef_ct(3) * dt_use, st.p, work);
+  stage<4>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  advance<4>(u, st, k);
+  mdx_rhs(u, t_end, st.p, work);
+  stage<5>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) u[j] += (double)k[5][j];
+  mdx_rhs(u, t_end, st.p, work);
+  stage<6>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) u[j] += (double)k[6][j];
+  mdx_rhs(u, t_end, st.p, work);
+  stage<7>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+
+  // Weighted RMS of the embedded error estimate k8 (modax/rodas5P.py:903-911).
+  double err_local = 0.0;
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) {
+    const double y_new_j = u[j] + (double)k[7][j];
+    const double scale = a.atol + a.rtol * pymax(fabs(st.y[j]), fabs(y_new_j));
+    const double r = weight(a, st.traj, j) * (double)k[7][j] / scale;
+    err_local += r * r;
+  }
+  const double err_norm = sqrt(err_local / MDX_NERR);
+  const bool accept = err_norm <= 1.0 && !isnan(err_norm);
+
+  double safe_err;
+  double factor = controller_factor(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2, MDX_E3,
+                                    MDX_USE_E2, MDX_USE_E3, safe_err);
+  if (accept) {
+    st.err_prev2 = st.err_prev;
+    st.err_prev = safe_err;
+  }
+  if (factor < FACTOR_MIN) factor = FACTOR_MIN;
+  else if (factor > FACTOR_MAX) factor = FACTOR_MAX;
+  st.dt = dt_use * factor;
+
+  if (accept) {
+#if MDX_CHECKPOINT
+    if (st.n_ckpt < a.ckpt_capacity) {
+      double* rec = a.ckpt + ((size_t)st.n_ckpt * (size_t)a.n_traj + (size_t)st.traj) * (MDX_NV + 2);
+      rec[0] = t;
+      rec[1] = dt_use;
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) rec[2 + j] = st.y[j];
+      ++st.n_ckpt;
+    } else {
+      st.ckpt_overflow = true;
+    }
+#endif
+    const double t_new = t + dt_use;
+    while (st.save_idx < a.n_save && save_reached(a.times[st.save_idx], t_new)) {
+      const double theta = (a.times[st.save_idx] - t) / dt_use;
+      const double theta1 = 1.0 - theta;
+#pragma unroll
+      for (int j = 0; j < MDX_NS; ++j) {
+        double h1 = coef_h(0, 0) * (double)k[0][j];
+        double h2 = coef_h(1, 0) * (double)k[0][j];
+        double h3 = coef_h(2, 0) * (double)k[0][j];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) {
+          h1 += coef_h(0, m) * (double)k[m][j];
+          h2 += coef_h(1, m) * (double)k[m][j];
+          h3 += coef_h(2, m) * (double)k[m][j];
+        }
+        const double y_new_j = u[j] + (double)k[7][j];
+        const double val = theta1 * st.y[j] + theta * (y_new_j + theta1 * (h1 + theta * (h2 + theta * h3)));
+#if MDX_SAVE_HISTORY
+        a.hist[hist_index(a, st.traj, st.save_idx, j)] = val;
+#endif
+      }
+      ++st.save_idx;
+    }
+#pragma unroll
+    for (int j = 0; j < MDX_NS; ++j) st.y[j] = u[j] + (double)k[7][j];
+    st.t += dt_use;
+    ++st.accepted;
+  } else {
+    ++st.rejected;
+  }
+  ++st.n_steps;
+}
+
+__device__ __forceinline__ void finish(State& st, const MdxSolveArgs& a) {
+  const bool hit_max = st.save_idx < a.n_save && st.t < st.tf_local;
+  // Save times past this trajectory's own end hold its final state
+  // (modax/rodas5P.py:991-1002).
+  while (st.save_idx < a.n_save) {
+#if MDX_SAVE_HISTORY
+#pragma unroll
+    for (int j = 0; j < MDX_NS; ++j) a.hist[hist_index(a, st.traj, st.save_idx, j)] = st.y[j];
+#endif
+    ++st.save_idx;
+  }
+#if !MDX_SAVE_HISTORY
+#pragma unroll
+  for (int j = 0; j < MDX_NS; ++j) a.hist[hist_index(a, st.traj, 0, j)] = st.y[j];
+#endif
+  a.accepted[st.traj] = st.accepted;
+  a.rejected[st.traj] = st.rejected;
+  a.loop_steps[st.traj] = st.n_steps;
+#if MDX_CHECKPOINT
+  if (a.ckpt_count) a.ckpt_count[st.traj] = st.n_ckpt;
+#endif
+  if (a.status) {
+    int status = hit_max ? MDX_STATUS_MAX_STEPS : MDX_STATUS_OK;
+#pragma unroll
+    for (int j = 0; j < MDX_NS; ++j)
+      if (!isfinite(st.y[j])) status |= MDX_STATUS_NONFINITE;
+#if MDX_CHECKPOINT
+    if (st.ckpt_overflow) status |= MDX_STATUS_CKPT_OVERFLOW;
+#endif
+    a.status[st.traj] = status;
+  }
+}
+
+}  // namespace rodas5p
+
+struct Rodas5P {
+  typedef rodas5p::State State;
+  static __device__ __forceinline__ void init(State& s, const MdxSolveArgs& a, int i) { rodas5p::init(s, a, i); }
+  static __device__ __forceinline__ bool running(const State& s, const MdxSolveArgs& a) { return rodas5p::running(s, a); }
+  static __device__ __forceinline__ void step(State& s, const MdxSolveArgs& a) { rodas5p::step(s, a); }
+  static __device__ __forceinline__ void finish(State& s, const MdxSolveArgs& a) { rodas5p::finish(s, a); }
+};
+
+}  // namespace mdx

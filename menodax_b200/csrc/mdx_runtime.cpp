@@ -1,0 +1,406 @@
+// menodax_b200 native runtime: NVRTC compilation, module lifetime and launches.
+//
+// Replaces the reference's native boundary, the XLA FFI handler that marshals
+// buffers and calls cuLaunchKernel on XLA's stream
+// (modax/_jax_numba_custom_call.py:66-231), and the ctypes cubin loader
+// (compile_kernel, modax/_jax_numba_custom_call.py:286-314).
+//
+// The CUDA driver is reached through dlopen("libcuda.so.1") and
+// cuGetProcAddress, resolved once under std::call_once, so the library loads on
+// a machine without a GPU (NVRTC compilation works there; launches return
+// MDX_E_NO_DRIVER).  A plan loads its cubin lazily, once per CUDA context.
+#include "../../include/menodax.h"
+#include "kernels/mdx_args.h"
+
+#include <cuda.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[2048];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+// --- driver entry points -------------------------------------------------------
+struct Driver {
+  bool ok = false;
+  std::string why;
+  decltype(&cuInit) init = nullptr;
+  decltype(&cuCtxGetCurrent) ctxGetCurrent = nullptr;
+  decltype(&cuCtxSetCurrent) ctxSetCurrent = nullptr;
+  decltype(&cuCtxGetDevice) ctxGetDevice = nullptr;
+  decltype(&cuDeviceGet) deviceGet = nullptr;
+  decltype(&cuDevicePrimaryCtxRetain) primaryCtxRetain = nullptr;
+  decltype(&cuDeviceGetAttribute) deviceGetAttribute = nullptr;
+  decltype(&cuModuleLoadData) moduleLoadData = nullptr;
+  decltype(&cuModuleUnload) moduleUnload = nullptr;
+  decltype(&cuModuleGetFunction) moduleGetFunction = nullptr;
+  decltype(&cuFuncSetAttribute) funcSetAttribute = nullptr;
+  decltype(&cuLaunchKernel) launchKernel = nullptr;
+  decltype(&cuMemsetD32Async) memsetD32Async = nullptr;
+  decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) occupancy = nullptr;
+  decltype(&cuGetErrorString) getErrorString = nullptr;
+};
+
+Driver g_driver;
+std::once_flag g_driver_once;
+
+typedef CUresult (*GetProcFn)(const char*, void**, int, cuuint64_t, CUdriverProcAddressQueryResult*);
+
+void load_driver() {
+  void* lib = dlopen("libcuda.so.1", RTLD_NOW | RTLD_GLOBAL);
+  if (!lib) {
+    g_driver.why = std::string("cannot load libcuda.so.1: ") + dlerror();
+    return;
+  }
+  GetProcFn get = (GetProcFn)dlsym(lib, "cuGetProcAddress_v2");
+  if (!get) {
+    g_driver.why = "libcuda.so.1 has no cuGetProcAddress_v2 (driver older than CUDA 12)";
+    return;
+  }
+  bool all = true;
+  auto resolve = [&](const char* name, void** slot) {
+    CUdriverProcAddressQueryResult q;
+    if (get(name, slot, 12000, CU_GET_PROC_ADDRESS_DEFAULT, &q) != CUDA_SUCCESS || !*slot) {
+      g_driver.why = std::string("driver symbol missing: ") + name;
+      all = false;
+    }
+  };
+  resolve("cuInit", (void**)&g_driver.init);
+  resolve("cuCtxGetCurrent", (void**)&g_driver.ctxGetCurrent);
+  resolve("cuCtxSetCurrent", (void**)&g_driver.ctxSetCurrent);
+  resolve("cuCtxGetDevice", (void**)&g_driver.ctxGetDevice);
+  resolve("cuDeviceGet", (void**)&g_driver.deviceGet);
+  resolve("cuDevicePrimaryCtxRetain", (void**)&g_driver.primaryCtxRetain);
+  resolve("cuDeviceGetAttribute", (void**)&g_driver.deviceGetAttribute);
+  resolve("cuModuleLoadData", (void**)&g_driver.moduleLoadData);
+  resolve("cuModuleUnload", (void**)&g_driver.moduleUnload);
+  resolve("cuModuleGetFunction", (void**)&g_driver.moduleGetFunction);
+  resolve("cuFuncSetAttribute", (void**)&g_driver.funcSetAttribute);
+  resolve("cuLaunchKernel", (void**)&g_driver.launchKernel);
+  resolve("cuMemsetD32Async", (void**)&g_driver.memsetD32Async);
+  resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&g_driver.occupancy);
+  resolve("cuGetErrorString", (void**)&g_driver.getErrorString);
+  if (!all) return;
+  if (g_driver.init(0) != CUDA_SUCCESS) {
+    g_driver.why = "cuInit failed (no usable GPU)";
+    return;
+  }
+  g_driver.ok = true;
+}
+
+int require_driver() {
+  std::call_once(g_driver_once, load_driver);
+  if (!g_driver.ok) return fail(MDX_E_NO_DRIVER, "%s", g_driver.why.c_str());
+  return MDX_OK;
+}
+
+int cuda_fail(CUresult r, const char* what) {
+  const char* s = nullptr;
+  if (g_driver.getErrorString) g_driver.getErrorString(r, &s);
+  return fail(MDX_E_CUDA, "%s failed: %s (%d)", what, s ? s : "unknown error", (int)r);
+}
+
+// The context launches go to: the calling thread's current one (torch makes the
+// device's primary context current), else device 0's primary context.
+int current_context(CUcontext* ctx) {
+  CUresult r = g_driver.ctxGetCurrent(ctx);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetCurrent");
+  if (*ctx) return MDX_OK;
+  CUdevice dev;
+  if ((r = g_driver.deviceGet(&dev, 0)) != CUDA_SUCCESS) return cuda_fail(r, "cuDeviceGet");
+  if ((r = g_driver.primaryCtxRetain(ctx, dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuDevicePrimaryCtxRetain");
+  if ((r = g_driver.ctxSetCurrent(*ctx)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxSetCurrent");
+  return MDX_OK;
+}
+
+struct Loaded {
+  CUmodule module = nullptr;
+  CUfunction plain = nullptr;
+  CUfunction persistent = nullptr;
+  CUfunction grad = nullptr;
+  int sm_count = 0;
+};
+
+}  // namespace
+
+struct mdx_plan {
+  mdx_plan_desc desc;
+  std::vector<char> cubin;
+  std::mutex mu;
+  std::unordered_map<CUcontext, Loaded> loaded;
+};
+
+namespace {
+
+int load_for_context(mdx_plan* plan, Loaded** out) {
+  int rc = require_driver();
+  if (rc) return rc;
+  CUcontext ctx;
+  if ((rc = current_context(&ctx))) return rc;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  auto it = plan->loaded.find(ctx);
+  if (it != plan->loaded.end()) {
+    *out = &it->second;
+    return MDX_OK;
+  }
+  Loaded l;
+  CUresult r = g_driver.moduleLoadData(&l.module, plan->cubin.data());
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuModuleLoadData");
+  if ((r = g_driver.moduleGetFunction(&l.plain, l.module, "mdx_solve_plain")) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuModuleGetFunction(mdx_solve_plain)");
+  if ((r = g_driver.moduleGetFunction(&l.persistent, l.module, "mdx_solve_persistent")) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuModuleGetFunction(mdx_solve_persistent)");
+  if (plan->desc.flags & MDX_PLAN_ADJOINT) {
+    if ((r = g_driver.moduleGetFunction(&l.grad, l.module, "mdx_grad_reverse")) != CUDA_SUCCESS)
+      return cuda_fail(r, "cuModuleGetFunction(mdx_grad_reverse)");
+  }
+  CUdevice dev;
+  if ((r = g_driver.ctxGetDevice(&dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
+  if ((r = g_driver.deviceGetAttribute(&l.sm_count, CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT, dev)) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuDeviceGetAttribute");
+  auto res = plan->loaded.emplace(ctx, l);
+  *out = &res.first->second;
+  return MDX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mdx_version(void) { return "menodax_b200 1.0 (abi 1)"; }
+
+int mdx_last_error(char* buf, size_t buf_size) {
+  if (buf && buf_size) {
+    size_t n = g_last_error.size() < buf_size - 1 ? g_last_error.size() : buf_size - 1;
+    memcpy(buf, g_last_error.data(), n);
+    buf[n] = '\0';
+  }
+  return (int)g_last_error.size();
+}
+
+void mdx_free(void* ptr) { free(ptr); }
+
+int mdx_compile(const char* source, const char* program_name, const char* const* options,
+                int n_options, void** cubin, size_t* cubin_size, char* log, size_t log_size) {
+  if (!source || !cubin || !cubin_size) return fail(MDX_E_INVALID, "mdx_compile: null argument");
+  if (n_options < 0 || (n_options > 0 && !options)) return fail(MDX_E_INVALID, "mdx_compile: bad options");
+  *cubin = nullptr;
+  *cubin_size = 0;
+  if (log && log_size) log[0] = '\0';
+  nvrtcProgram prog;
+  nvrtcResult r = nvrtcCreateProgram(&prog, source, program_name ? program_name : "mdx_problem.cu",
+                                     0, nullptr, nullptr);
+  if (r != NVRTC_SUCCESS) return fail(MDX_E_COMPILE, "nvrtcCreateProgram: %s", nvrtcGetErrorString(r));
+  r = nvrtcCompileProgram(prog, n_options, options);
+  size_t n_log = 0;
+  nvrtcGetProgramLogSize(prog, &n_log);
+  std::string text(n_log, '\0');
+  if (n_log) nvrtcGetProgramLog(prog, &text[0]);
+  if (log && log_size) {
+    size_t n = text.size() < log_size - 1 ? text.size() : log_size - 1;
+    memcpy(log, text.data(), n);
+    log[n] = '\0';
+  }
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    return fail(MDX_E_COMPILE, "NVRTC: %s\n%s", nvrtcGetErrorString(r), text.c_str());
+  }
+  size_t n = 0;
+  r = nvrtcGetCUBINSize(prog, &n);
+  if (r != NVRTC_SUCCESS || n == 0) {
+    nvrtcDestroyProgram(&prog);
+    return fail(MDX_E_COMPILE, "NVRTC produced no cubin (was -arch=sm_100a given?)");
+  }
+  void* buf = malloc(n);
+  if (!buf) {
+    nvrtcDestroyProgram(&prog);
+    return fail(MDX_E_NOMEM, "out of host memory for the cubin");
+  }
+  nvrtcGetCUBIN(prog, (char*)buf);
+  nvrtcDestroyProgram(&prog);
+  *cubin = buf;
+  *cubin_size = n;
+  return MDX_OK;
+}
+
+int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
+  if (!desc || !plan) return fail(MDX_E_INVALID, "mdx_plan_create: null argument");
+  if (desc->struct_size != (int)sizeof(mdx_plan_desc))
+    return fail(MDX_E_INVALID, "mdx_plan_desc.struct_size %d != %d", desc->struct_size, (int)sizeof(mdx_plan_desc));
+  if (desc->solver != MDX_SOLVER_TSIT5 && desc->solver != MDX_SOLVER_RODAS5P)
+    return fail(MDX_E_INVALID, "unknown solver %d", desc->solver);
+  if (desc->n_vars <= 0 || desc->n_system < desc->n_vars || desc->n_params < 0)
+    return fail(MDX_E_INVALID, "bad sizes n_vars=%d n_system=%d n_params=%d", desc->n_vars, desc->n_system, desc->n_params);
+  if (desc->threads_per_block <= 0 || desc->threads_per_block % 32 != 0 || desc->threads_per_block > 1024)
+    return fail(MDX_E_INVALID, "threads_per_block must be a multiple of 32 in [32, 1024]; got %d", desc->threads_per_block);
+  if (!desc->cubin || desc->cubin_size == 0) return fail(MDX_E_INVALID, "mdx_plan_create: empty cubin");
+  mdx_plan* p = new (std::nothrow) mdx_plan;
+  if (!p) return fail(MDX_E_NOMEM, "out of host memory");
+  p->desc = *desc;
+  p->cubin.assign((const char*)desc->cubin, (const char*)desc->cubin + desc->cubin_size);
+  p->desc.cubin = nullptr;
+  *plan = p;
+  return MDX_OK;
+}
+
+int mdx_plan_destroy(mdx_plan* plan) {
+  if (!plan) return MDX_OK;
+  if (g_driver.ok) {
+    for (auto& kv : plan->loaded)
+      if (kv.second.module) g_driver.moduleUnload(kv.second.module);
+  }
+  delete plan;
+  return MDX_OK;
+}
+
+int mdx_workspace_size(const mdx_plan* plan, int mode, int n_traj, size_t* bytes) {
+  if (!plan || !bytes) return fail(MDX_E_INVALID, "mdx_workspace_size: null argument");
+  if (n_traj < 0) return fail(MDX_E_INVALID, "n_traj must be non-negative");
+  *bytes = mode == MDX_LAUNCH_PERSISTENT ? 256 : 0;
+  return MDX_OK;
+}
+
+int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count) {
+  if (!plan || !blocks_per_sm || !sm_count) return fail(MDX_E_INVALID, "mdx_occupancy: null argument");
+  Loaded* l;
+  int rc = load_for_context(plan, &l);
+  if (rc) return rc;
+  CUfunction f = mode == MDX_LAUNCH_PERSISTENT ? l->persistent : l->plain;
+  CUresult r = g_driver.occupancy(blocks_per_sm, f, plan->desc.threads_per_block, 0);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  *sm_count = l->sm_count;
+  return MDX_OK;
+}
+
+int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
+  if (!plan || !d) return fail(MDX_E_INVALID, "mdx_solve: null argument");
+  if (d->struct_size != (int)sizeof(mdx_solve_desc))
+    return fail(MDX_E_INVALID, "mdx_solve_desc.struct_size %d != %d", d->struct_size, (int)sizeof(mdx_solve_desc));
+  if (d->n_traj < 0) return fail(MDX_E_INVALID, "n_traj must be non-negative; got %d", d->n_traj);
+  if (d->n_save < 1) return fail(MDX_E_INVALID, "times must hold at least one value; got %d", d->n_save);
+  if (d->n_save_hist != d->n_save && d->n_save_hist != 1)
+    return fail(MDX_E_INVALID, "n_save_hist must be n_save or 1; got %d", d->n_save_hist);
+  if (d->mode != MDX_LAUNCH_PLAIN && d->mode != MDX_LAUNCH_PERSISTENT)
+    return fail(MDX_E_INVALID, "unknown launch mode %d", d->mode);
+  if (d->n_traj == 0) return MDX_OK;
+  if (!d->y0 || !d->times || (plan->desc.n_params > 0 && !d->params) || !d->hist || !d->accepted ||
+      !d->rejected || !d->loop_steps)
+    return fail(MDX_E_INVALID, "mdx_solve: a required buffer is NULL");
+  const bool ckpt = (plan->desc.flags & MDX_PLAN_CHECKPOINT) != 0;
+  if (ckpt && (!d->ckpt || !d->ckpt_count || d->ckpt_capacity < 1))
+    return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt, ckpt_count and ckpt_capacity >= 1");
+  if (d->mode == MDX_LAUNCH_PERSISTENT && (!d->workspace || d->workspace_bytes < 4))
+    return fail(MDX_E_INVALID, "the persistent launch needs a workspace of at least 4 bytes");
+
+  Loaded* l;
+  int rc = load_for_context(plan, &l);
+  if (rc) return rc;
+
+  MdxSolveArgs a;
+  memset(&a, 0, sizeof(a));
+  a.y0 = d->y0;
+  a.times = d->times;
+  a.params = d->params;
+  a.weights = d->weights;
+  a.hist = d->hist;
+  a.accepted = d->accepted;
+  a.rejected = d->rejected;
+  a.loop_steps = d->loop_steps;
+  a.status = d->status;
+  a.hook_out = d->hook_out;
+  a.order = d->order;
+  a.ckpt = ckpt ? d->ckpt : nullptr;
+  a.ckpt_count = ckpt ? d->ckpt_count : nullptr;
+  a.ckpt_capacity = ckpt ? d->ckpt_capacity : 0;
+  a.n_traj = d->n_traj;
+  a.n_save = d->n_save;
+  a.n_save_hist = d->n_save_hist;
+  a.max_steps = d->max_steps;
+  a.dt0 = d->dt0;
+  a.rtol = d->rtol;
+  a.atol = d->atol;
+
+  const unsigned tpb = (unsigned)plan->desc.threads_per_block;
+  CUstream s = (CUstream)stream;
+  CUfunction f;
+  unsigned grid;
+  if (d->mode == MDX_LAUNCH_PLAIN) {
+    f = l->plain;
+    grid = (unsigned)((d->n_traj + tpb - 1) / tpb);
+  } else {
+    f = l->persistent;
+    a.work_counter = (int*)d->workspace;
+    int blocks = d->grid_blocks;
+    if (blocks <= 0) {
+      int per_sm = 0;
+      CUresult r = g_driver.occupancy(&per_sm, f, (int)tpb, 0);
+      if (r != CUDA_SUCCESS) return cuda_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+      if (per_sm < 1) per_sm = 1;
+      blocks = per_sm * l->sm_count;
+    }
+    const int needed = (d->n_traj + (int)tpb - 1) / (int)tpb;
+    if (blocks > needed) blocks = needed;
+    grid = (unsigned)blocks;
+    CUresult r = g_driver.memsetD32Async((CUdeviceptr)d->workspace, 0u, 1, s);
+    if (r != CUDA_SUCCESS) return cuda_fail(r, "cuMemsetD32Async(work counter)");
+  }
+  void* params[] = {&a};
+  CUresult r = g_driver.launchKernel(f, grid, 1, 1, tpb, 1, 1, 0, s, params, nullptr);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_solve)");
+  return MDX_OK;
+}
+
+int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
+  if (!plan || !d) return fail(MDX_E_INVALID, "mdx_grad: null argument");
+  if (d->struct_size != (int)sizeof(mdx_grad_desc))
+    return fail(MDX_E_INVALID, "mdx_grad_desc.struct_size %d != %d", d->struct_size, (int)sizeof(mdx_grad_desc));
+  if (!(plan->desc.flags & MDX_PLAN_ADJOINT)) return fail(MDX_E_INVALID, "the plan was built without the adjoint kernel");
+  if (d->n_traj < 0 || d->n_save < 1) return fail(MDX_E_INVALID, "bad sizes n_traj=%d n_save=%d", d->n_traj, d->n_save);
+  if (d->n_traj == 0) return MDX_OK;
+  if (!d->times || !d->ckpt || !d->ckpt_count || !d->grad_hist || !d->grad_y0 || !d->grad_params ||
+      d->ckpt_capacity < 1)
+    return fail(MDX_E_INVALID, "mdx_grad: a required buffer is NULL");
+  Loaded* l;
+  int rc = load_for_context(plan, &l);
+  if (rc) return rc;
+  MdxGradArgs a;
+  memset(&a, 0, sizeof(a));
+  a.times = d->times;
+  a.params = d->params;
+  a.ckpt = d->ckpt;
+  a.ckpt_count = d->ckpt_count;
+  a.grad_hist = d->grad_hist;
+  a.grad_y0 = d->grad_y0;
+  a.grad_params = d->grad_params;
+  a.status = d->status;
+  a.ckpt_capacity = d->ckpt_capacity;
+  a.n_traj = d->n_traj;
+  a.n_save = d->n_save;
+  const unsigned tpb = (unsigned)plan->desc.threads_per_block;
+  const unsigned grid = (unsigned)((d->n_traj + tpb - 1) / tpb);
+  void* params[] = {&a};
+  CUresult r = g_driver.launchKernel(l->grad, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_reverse)");
+  return MDX_OK;
+}
+
+}  // extern "C"

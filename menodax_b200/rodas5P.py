@@ -1,0 +1,119 @@
+"""Rodas5P ensemble solve: the drop-in for ``modax.rodas5P.solve``.
+
+Same signature and defaults as ``modax/rodas5P.py:1024-1051``, same errors
+(``modax/rodas5P.py:1204-1211``), same outputs: ``hist (N, S, n_vars)`` or
+``(hist, stats)``.  Extra keyword ``launch`` picks the one-launch kernel
+(``"plain"``), the persistent refill kernel (``"persistent"``) or lets the
+library choose (``"auto"``).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from menodax_b200._frontend import run
+from menodax_b200._problem import KernelOptions
+from menodax_b200._sparsity import normalize_sparsity
+
+_DEFAULT_TRAJECTORIES_PER_BLOCK = 32
+LU_PRECISIONS = ("fp32", "fp64")
+
+
+def trajectories_per_block_or_default(requested=None) -> int:
+    """Trajectories a block carries, one per thread (``modax/rodas5P.py:118-134``)."""
+    if requested is None:
+        return _DEFAULT_TRAJECTORIES_PER_BLOCK
+    requested = int(requested)
+    if requested < 1:
+        raise ValueError(f"trajectories_per_block must be positive, got {requested}")
+    return requested
+
+
+def _block_size(requested: int) -> int:
+    # Warp ballots need whole warps, so a block is rounded up to them.
+    return max(32, (requested + 31) // 32 * 32)
+
+
+def solve(
+    ode_fn,
+    y0,
+    t_span,
+    params,
+    *,
+    rtol=1e-8,
+    atol=1e-10,
+    first_step=None,
+    max_steps=100000,
+    return_stats=False,
+    error_weights=None,
+    pcoeff=0.0,
+    icoeff=1.0,
+    dcoeff=0.0,
+    lu_precision: str = "fp32",
+    trajectories_per_block=None,
+    sens_error_control=True,
+    sens_param_columns=None,
+    sparsity=None,
+    ordering="amd",
+    tf_index=None,
+    max_registers=None,
+    array_rhs=None,
+    save_hook=None,
+    hook_size: int = 0,
+    save_history: bool = True,
+    launch: str = "auto",
+):
+    """Rodas5P ensemble solve of ``y' = ode_fn(y, t, p)`` on one GPU.
+
+    ``lu_precision`` selects the precision of the iteration matrix, its LU and
+    the stored stage increments; the state, right-hand side, Jacobian, error and
+    controller are always double.  ``sparsity`` (a mask, a scipy sparse matrix or
+    ``(nnz, 2)`` pairs) colours the Jacobian sweep and compiles a sparse LU for the
+    pattern, ordered by ``ordering`` (``"amd"`` or ``"natural"``).  ``tf_index``
+    names a parameter column holding each trajectory's own end time.
+
+    Torch inputs that require grad are differentiated by the discrete adjoint
+    (checkpointed step states, reverse sweep on the device).
+    """
+    if lu_precision not in LU_PRECISIONS:
+        raise ValueError(f"lu_precision must be one of {LU_PRECISIONS}; got {lu_precision!r}")
+    if array_rhs is not None:
+        raise NotImplementedError(
+            "array_rhs is a numba device function; this build traces ode_fn itself "
+            "and needs no separate array form"
+        )
+    if save_hook is not None:
+        if hook_size <= 0:
+            raise ValueError("a save_hook needs a positive hook_size")
+        raise NotImplementedError("save_hook is not supported by this build")
+    if not save_history:
+        raise ValueError("save_history=False needs a save_hook to consume the saves")
+    n_vars = int(torch.as_tensor(y0).shape[-1]) if not hasattr(y0, "shape") else int(y0.shape[-1])
+    if sparsity is not None:
+        sparsity = normalize_sparsity(sparsity, n_vars)
+    tpb = trajectories_per_block_or_default(trajectories_per_block)
+    options = KernelOptions(
+        solver="rodas5P",
+        pcoeff=float(pcoeff),
+        icoeff=float(icoeff),
+        dcoeff=float(dcoeff),
+        lu_precision=lu_precision,
+        threads_per_block=_block_size(tpb),
+        sparsity=sparsity,
+        ordering=ordering,
+        tf_index=-1 if tf_index is None else int(tf_index),
+        max_registers=max_registers,
+        save_history=bool(save_history),
+    )
+    from menodax_b200.autograd import needs_grad, solve_with_grad
+
+    if needs_grad(y0, params):
+        return solve_with_grad(
+            ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
+            max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
+        )
+    return run(
+        ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
+        max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
+        launch_mode=launch,
+    )

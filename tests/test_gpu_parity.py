@@ -1,0 +1,118 @@
+"""GPU parity: the sm_100a kernels against the CPU oracle on the same seeded inputs.
+
+The bar (FP64 path): saved states agree within 1e-9 relative and the step
+counts are identical on at least 99.9% of trajectories.  FP32-LU path: within
+10 * rtol of an FP64 oracle solved at rtol = 1e-12.  The plain one-launch and
+the persistent refill kernels run the same per-trajectory arithmetic, so they
+must agree bit for bit.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from menodax_b200 import rodas5P, systems, tsit5
+
+pytestmark = pytest.mark.gpu
+
+
+def _states_agree(gpu, ora, same_steps, rtol=1e-9, atol=1e-14):
+    g = np.asarray(gpu)[same_steps]
+    o = np.asarray(ora)[same_steps]
+    np.testing.assert_allclose(g, o, rtol=rtol, atol=atol)
+
+
+def _step_match(gpu_stats, acc, rej):
+    ga = np.asarray(gpu_stats["accepted_steps"])
+    gr = np.asarray(gpu_stats["rejected_steps"])
+    same = (ga == acc) & (gr == rej)
+    return same
+
+
+def test_tsit5_lorenz_matches_oracle(oracle):
+    cfg = systems.lorenz_config(size=1024)
+    hist, stats = tsit5.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"],
+                              rtol=cfg["rtol"], atol=cfg["atol"], return_stats=True)
+    h, a, r, l = oracle.solve("tsit5", oracle.System.lorenz(), cfg["y0"], cfg["t_span"], cfg["params"],
+                              rtol=cfg["rtol"], atol=cfg["atol"])
+    same = _step_match(stats, a, r)
+    assert same.mean() >= 0.999
+    _states_agree(hist, h, same)
+
+
+def test_tsit5_lorenz_golden_step_counts(oracle):
+    """722 attempted / 104 rejected (benchmarks/nonstiff_lorenz_divergence CSV row 2)."""
+    y0, p = systems.lorenz_divergence_scenario(64, divergence=0.0)
+    _, stats = tsit5.solve(systems.lorenz, y0, (0.0, 5.0), p, rtol=1e-6, atol=1e-8,
+                           first_step=1e-4, return_stats=True)
+    assert (np.asarray(stats["loop_steps"]) == 722).all()
+    assert (np.asarray(stats["rejected_steps"]) == 104).all()
+
+
+def test_tsit5_lorenz_divergence_distribution():
+    """Divergence 0.1 at 100k trajectories: mean 699.81274, min 664, max 735, rejected 102.78706."""
+    y0, p = systems.lorenz_divergence_scenario(100_000, divergence=0.1)
+    _, stats = tsit5.solve(systems.lorenz, y0, (0.0, 5.0), p, rtol=1e-6, atol=1e-8,
+                           first_step=1e-4, return_stats=True)
+    loop = np.asarray(stats["loop_steps"])
+    assert abs(loop.mean() - 699.81274) < 0.01
+    assert loop.min() == 664 and loop.max() == 735
+
+
+@pytest.mark.parametrize("lu_precision", ["fp64", "fp32"])
+def test_rodas5p_robertson_matches_oracle(oracle, lu_precision):
+    cfg = systems.robertson_config(size=2048)
+    hist, stats = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"],
+                                rtol=cfg["rtol"], atol=cfg["atol"], lu_precision=lu_precision,
+                                return_stats=True, launch="plain")
+    h, a, r, l = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"],
+                              cfg["params"], rtol=cfg["rtol"], atol=cfg["atol"], lu_precision=lu_precision)
+    same = _step_match(stats, a, r)
+    if lu_precision == "fp64":
+        assert same.mean() >= 0.999
+        _states_agree(hist, h, same, atol=1e-15)
+    else:
+        assert same.mean() >= 0.95
+
+
+def test_rodas5p_robertson_fp32_within_10_rtol_of_fp64_oracle(oracle):
+    cfg = systems.robertson_config(size=1024)
+    hist = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"],
+                         atol=cfg["atol"], lu_precision="fp32")
+    ref, *_ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
+                           rtol=1e-12, atol=1e-16, lu_precision="fp64")
+    err = np.abs(hist - ref) / (np.abs(ref) + cfg["atol"] / cfg["rtol"])
+    assert err.max() <= 10 * cfg["rtol"]
+
+
+def test_rodas5p_robertson_golden_fp32_steps():
+    """157 attempted / 10 rejected (benchmarks/stiff_robertson_divergence CSV row 2)."""
+    n = 64
+    y0 = np.broadcast_to(systems.ROBERTSON_Y0, (n, 3)).copy()
+    p = np.broadcast_to(systems.ROBERTSON_PARAMS, (n, 3)).copy()
+    _, stats = rodas5P.solve(systems.robertson, y0, systems.ROBERTSON_TIMES, p, rtol=1e-6, atol=1e-8,
+                             first_step=1e-4, lu_precision="fp32", return_stats=True)
+    loop = np.asarray(stats["loop_steps"])
+    rej = np.asarray(stats["rejected_steps"])
+    assert abs(int(loop[0]) - 157) <= 1 and abs(int(rej[0]) - 10) <= 1
+
+
+@pytest.mark.parametrize("lu_precision", ["fp64", "fp32"])
+def test_persistent_kernel_is_bit_identical_to_plain(lu_precision):
+    cfg = systems.robertson_config(size=5000)
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision=lu_precision, return_stats=True)
+    h1, s1 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], launch="plain", **kw)
+    h2, s2 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], launch="persistent", **kw)
+    assert np.array_equal(h1, h2)
+    for k in s1:
+        assert np.array_equal(s1[k], s2[k])
+
+
+def test_torch_device_inputs_stay_on_device():
+    cfg = systems.lorenz_config(size=256)
+    y0 = torch.as_tensor(cfg["y0"], device="cuda")
+    p = torch.as_tensor(cfg["params"], device="cuda")
+    out = tsit5.solve(cfg["ode_fn"], y0, cfg["t_span"], p, rtol=cfg["rtol"], atol=cfg["atol"])
+    assert isinstance(out, torch.Tensor) and out.is_cuda
+    ref = tsit5.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"], atol=cfg["atol"])
+    assert np.array_equal(out.cpu().numpy(), ref)

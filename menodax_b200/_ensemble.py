@@ -98,16 +98,20 @@ def to_device(t, device):
 
 
 class Workspace:
-    """Per-device scratch the persistent launch needs (the queue head), reused across calls."""
+    """Scratch the persistent launch needs (the queue head), one per (device, stream).
 
-    _by_device: dict = {}
+    Launches on one stream are ordered, so they may share one; launches on two
+    streams may overlap, so each stream gets its own."""
+
+    _by_stream: dict = {}
 
     @classmethod
-    def get(cls, device, nbytes: int):
-        buf = cls._by_device.get(device)
+    def get(cls, device, stream: int, nbytes: int):
+        key = (device, stream)
+        buf = cls._by_stream.get(key)
         if buf is None or buf.numel() < nbytes:
             buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
-            cls._by_device[device] = buf
+            cls._by_stream[key] = buf
         return buf
 
 
@@ -117,7 +121,8 @@ def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, m
     """Allocate outputs on ``y0``'s device and launch one ensemble solve.
 
     All inputs must already be contiguous float64 CUDA tensors on one device.
-    Returns ``(hist, accepted, rejected, loop_steps, status)``.
+    Returns ``(hist, counters)``; the rows of ``counters`` (4, N) int32 are the
+    accepted, rejected and attempted step counts and the status bits.
     """
     n = y0.shape[0]
     n_save = times.shape[0]
@@ -147,9 +152,10 @@ def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, m
     desc.loop_steps = counters[2].data_ptr()
     desc.status = counters[3].data_ptr()
     desc.order = order.data_ptr() if order is not None else None
+    stream = torch.cuda.current_stream(dev).cuda_stream
     if mode == _native.MDX_LAUNCH_PERSISTENT:
         nbytes = problem.plan.workspace_size(mode, n)
-        ws = Workspace.get(dev, nbytes)
+        ws = Workspace.get(dev, stream, nbytes)
         desc.workspace = ws.data_ptr()
         desc.workspace_bytes = ws.numel()
     desc.grid_blocks = int(grid_blocks)
@@ -157,7 +163,6 @@ def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, m
         desc.ckpt = ckpt.data_ptr()
         desc.ckpt_count = ckpt_count.data_ptr()
         desc.ckpt_capacity = int(ckpt_capacity)
-    stream = torch.cuda.current_stream(dev).cuda_stream
     with torch.cuda.device(dev):
         problem.plan.solve(desc, stream)
-    return hist, counters[0], counters[1], counters[2], counters[3]
+    return hist, counters

@@ -74,24 +74,35 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     p_d = to_device(p_t.detach(), device)
     t_d = to_device(times, device)
     w_d = to_device(weights.detach(), device) if weights is not None else None
-    hist, acc, rej, loop, status = launch(
+    hist, counters = launch(
         problem, y0=y0_d, times=t_d, params=p_d, weights=w_d, dt0=initial_step(first_step),
         rtol=rtol, atol=atol, max_steps=max_steps, mode=mode,
         n_save_hist=None if options.save_history else 1, grid_blocks=grid_blocks,
     )
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     if torch_io and input_on_gpu:
-        out = (hist,)
-        stats = solver_stats(acc, rej, loop)
-    elif torch_io:
-        out = (hist.cpu(),)
-        stats = solver_stats(acc.cpu(), rej.cpu(), loop.cpu())
-    else:
-        out = (hist.cpu().numpy(),)
-        stats = solver_stats(acc.cpu().numpy(), rej.cpu().numpy(), loop.cpu().numpy())
+        if return_stats:
+            return hist, solver_stats(counters[0], counters[1], counters[2])
+        return hist
+    hist_h, counters_h = _to_host(hist, counters[:3] if return_stats else None)
+    if not torch_io:
+        hist_h = hist_h.numpy()
+        counters_h = counters_h.numpy() if counters_h is not None else None
     if return_stats:
-        return out[0], stats
-    return out[0]
+        return hist_h, solver_stats(counters_h[0], counters_h[1], counters_h[2])
+    return hist_h
+
+
+def _to_host(hist, counters):
+    """Device -> pinned host copies (torch's caching host allocator), one sync."""
+    hist_h = torch.empty(hist.shape, dtype=hist.dtype, pin_memory=True)
+    hist_h.copy_(hist, non_blocking=True)
+    counters_h = None
+    if counters is not None:
+        counters_h = torch.empty(counters.shape, dtype=counters.dtype, pin_memory=True)
+        counters_h.copy_(counters, non_blocking=True)
+    torch.cuda.current_stream(hist.device).synchronize()
+    return hist_h, counters_h
 
 
 def _replace(options, **kw):

@@ -142,6 +142,19 @@ int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count);
 /* Launch one ensemble solve on `stream`.  Asynchronous. */
 int mdx_solve(mdx_plan* plan, const mdx_solve_desc* desc, void* stream);
 
+/* The persistent refill solve for callers that cannot allocate device memory
+ * (a plugin or custom-call handler that owns only its inputs and outputs, a
+ * host whose allocator must not be bypassed).  No counterpart in the reference.
+ * Same as mdx_solve with MDX_LAUNCH_PERSISTENT, except that the work-queue
+ * scratch comes from a MDX_NOALLOC_SCRATCH_BYTES array inside the library on
+ * each GPU (held until exit) instead of desc->workspace, which is ignored; a solve
+ * needing more scratch than that is rejected with MDX_E_INVALID.  It calls no
+ * allocator.  The first call on a device looks up the array's address (make it
+ * before any stream capture); calls share the array, so calls whose kernels
+ * overlap on the GPU race.  Needs the device's primary context current. */
+#define MDX_NOALLOC_SCRATCH_BYTES 4096
+int mdx_solve_persistent_noalloc(mdx_plan* plan, const mdx_solve_desc* desc, void* stream);
+
 /* Launch the discrete-adjoint reverse pass on `stream` (MDX_PLAN_ADJOINT plans). */
 int mdx_grad(mdx_plan* plan, const mdx_grad_desc* desc, void* stream);
 

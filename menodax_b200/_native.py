@@ -38,7 +38,7 @@ MDX_STATUS_CKPT_OVERFLOW = 4
 EXPORTED = (
     "mdx_compile", "mdx_free", "mdx_plan_create", "mdx_plan_destroy", "mdx_workspace_size",
     "mdx_occupancy", "mdx_solve", "mdx_grad", "mdx_last_error", "mdx_version",
-    "mdx_measure_fma_peak",
+    "mdx_measure_fma_peak", "mdx_solve_persistent_noalloc",
 )
 
 
@@ -81,8 +81,8 @@ class GradDesc(ctypes.Structure):
 
 
 def _library_sources():
-    return [CSRC / "mdx_runtime.cpp", CSRC / "mdx_peak.cu", KERNEL_DIR / "mdx_args.h",
-            INCLUDE_DIR / "menodax.h"]
+    return [CSRC / "mdx_runtime.cpp", CSRC / "mdx_peak.cu", CSRC / "mdx_noalloc.cu",
+            CSRC / "mdx_internal.h", KERNEL_DIR / "mdx_args.h", INCLUDE_DIR / "menodax.h"]
 
 
 def build_library(force: bool = False) -> Path:
@@ -95,6 +95,7 @@ def build_library(force: bool = False) -> Path:
     cmd = [
         str(CUDA_HOME / "bin" / "nvcc"), "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
         "-Xcompiler", "-Wall", f"-I{CUDA_HOME / 'include'}", str(CSRC / "mdx_runtime.cpp"), str(CSRC / "mdx_peak.cu"),
+        str(CSRC / "mdx_noalloc.cu"),
         "-o", str(LIB_PATH), f"-L{CUDA_HOME / 'lib64'}", "-lnvrtc", "-ldl",
         f"-Xlinker=-rpath,{CUDA_HOME / 'lib64'}",
     ]
@@ -135,6 +136,7 @@ def lib():
         L.mdx_grad.argtypes = [ctypes.c_void_p, ctypes.POINTER(GradDesc), ctypes.c_void_p]
         L.mdx_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         L.mdx_version.restype = ctypes.c_char_p
+        L.mdx_solve_persistent_noalloc.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveDesc), ctypes.c_void_p]
         L.mdx_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         _lib = L
         return _lib

@@ -11,6 +11,7 @@
 // MDX_E_NO_DRIVER).  A plan loads its cubin lazily, once per CUDA context.
 #include "../../include/menodax.h"
 #include "kernels/mdx_args.h"
+#include "mdx_internal.h"
 
 #include <cuda.h>
 #include <dlfcn.h>
@@ -49,6 +50,7 @@ struct Driver {
   decltype(&cuCtxGetDevice) ctxGetDevice = nullptr;
   decltype(&cuDeviceGet) deviceGet = nullptr;
   decltype(&cuDevicePrimaryCtxRetain) primaryCtxRetain = nullptr;
+  decltype(&cuDevicePrimaryCtxRelease) primaryCtxRelease = nullptr;
   decltype(&cuDeviceGetAttribute) deviceGetAttribute = nullptr;
   decltype(&cuModuleLoadData) moduleLoadData = nullptr;
   decltype(&cuModuleUnload) moduleUnload = nullptr;
@@ -90,6 +92,7 @@ void load_driver() {
   resolve("cuCtxGetDevice", (void**)&g_driver.ctxGetDevice);
   resolve("cuDeviceGet", (void**)&g_driver.deviceGet);
   resolve("cuDevicePrimaryCtxRetain", (void**)&g_driver.primaryCtxRetain);
+  resolve("cuDevicePrimaryCtxRelease", (void**)&g_driver.primaryCtxRelease);
   resolve("cuDeviceGetAttribute", (void**)&g_driver.deviceGetAttribute);
   resolve("cuModuleLoadData", (void**)&g_driver.moduleLoadData);
   resolve("cuModuleUnload", (void**)&g_driver.moduleUnload);
@@ -291,7 +294,13 @@ int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count) {
   return MDX_OK;
 }
 
-int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
+}  // extern "C"
+
+namespace mdx_internal {
+
+// The body of mdx_solve.  `counter` (when not NULL) replaces the caller's
+// workspace as the persistent kernel's queue head.
+int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, int* counter) {
   if (!plan || !d) return fail(MDX_E_INVALID, "mdx_solve: null argument");
   if (d->struct_size != (int)sizeof(mdx_solve_desc))
     return fail(MDX_E_INVALID, "mdx_solve_desc.struct_size %d != %d", d->struct_size, (int)sizeof(mdx_solve_desc));
@@ -308,7 +317,7 @@ int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
   const bool ckpt = (plan->desc.flags & MDX_PLAN_CHECKPOINT) != 0;
   if (ckpt && (!d->ckpt || !d->ckpt_count || d->ckpt_capacity < 1))
     return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt, ckpt_count and ckpt_capacity >= 1");
-  if (d->mode == MDX_LAUNCH_PERSISTENT && (!d->workspace || d->workspace_bytes < 4))
+  if (d->mode == MDX_LAUNCH_PERSISTENT && !counter && (!d->workspace || d->workspace_bytes < 4))
     return fail(MDX_E_INVALID, "the persistent launch needs a workspace of at least 4 bytes");
 
   Loaded* l;
@@ -348,7 +357,7 @@ int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
     grid = (unsigned)((d->n_traj + tpb - 1) / tpb);
   } else {
     f = l->persistent;
-    a.work_counter = (int*)d->workspace;
+    a.work_counter = counter ? counter : (int*)d->workspace;
     int blocks = d->grid_blocks;
     if (blocks <= 0) {
       int per_sm = 0;
@@ -360,13 +369,40 @@ int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
     const int needed = (d->n_traj + (int)tpb - 1) / (int)tpb;
     if (blocks > needed) blocks = needed;
     grid = (unsigned)blocks;
-    CUresult r = g_driver.memsetD32Async((CUdeviceptr)d->workspace, 0u, 1, s);
+    CUresult r = g_driver.memsetD32Async((CUdeviceptr)a.work_counter, 0u, 1, s);
     if (r != CUDA_SUCCESS) return cuda_fail(r, "cuMemsetD32Async(work counter)");
   }
   void* params[] = {&a};
   CUresult r = g_driver.launchKernel(f, grid, 1, 1, tpb, 1, 1, 0, s, params, nullptr);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_solve)");
   return MDX_OK;
+}
+
+int current_device(int* device, bool* is_primary) {
+  int rc = require_driver();
+  if (rc) return rc;
+  CUcontext ctx;
+  CUresult r = g_driver.ctxGetCurrent(&ctx);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetCurrent");
+  if (!ctx) return fail(MDX_E_INVALID, "no CUDA context is current on this thread");
+  CUdevice dev;
+  if ((r = g_driver.ctxGetDevice(&dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
+  CUcontext primary;
+  if ((r = g_driver.primaryCtxRetain(&primary, dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuDevicePrimaryCtxRetain");
+  g_driver.primaryCtxRelease(dev);
+  *device = (int)dev;
+  *is_primary = primary == ctx;
+  return MDX_OK;
+}
+
+int fail_message(int code, const char* message) { return fail(code, "%s", message); }
+
+}  // namespace mdx_internal
+
+extern "C" {
+
+int mdx_solve(mdx_plan* plan, const mdx_solve_desc* d, void* stream) {
+  return mdx_internal::solve_with_counter(plan, d, stream, nullptr);
 }
 
 int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {

@@ -167,7 +167,10 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         parts.append("#define MDX_SOLVER mdx::Tsit5")
     parts.append('#include "mdx_entry.cuh"')
     if options.adjoint:
+        if sens is not None:
+            raise ValueError("the discrete adjoint differentiates the plain solve; drop sens")
         parts.append(emit_adjoint_pieces(tr))
+        parts.append("#define MDX_ADJOINT_RODAS5P" if rodas else "#define MDX_ADJOINT_TSIT5")
         parts.append('#include "mdx_adjoint.cuh"')
     meta = dict(n_system=n_system, n_error=n_error, lu_size=lu_size, sparse=sparse)
     return "\n".join(parts) + "\n", meta

@@ -22,6 +22,7 @@ folding a literal seed does for ``modax`` after inlining (``modax/rodas5P.py:480
 from __future__ import annotations
 
 import math
+import operator
 import types
 from dataclasses import dataclass
 
@@ -425,7 +426,7 @@ class _Vector:
         if isinstance(index, slice):
             return [self[i] for i in range(*index.indices(self._size))]
         try:
-            i = int(index)
+            i = operator.index(index)
         except TypeError:
             raise TraceError(
                 f"{self._kind}[...] must be indexed with an integer literal"

@@ -1,0 +1,353 @@
+// Discrete adjoint of a checkpointed ensemble solve, one trajectory per thread.
+//
+// The forward solve (MDX_CHECKPOINT) records, for every accepted step m, the
+// step state (t_m, h_m, y_m).  This kernel walks the steps backwards: it
+// recomputes step m from its state -- Jacobian, df/dt, LU and the eight stages
+// (Rodas5P) or the seven stages (Tsit5) -- then back-propagates the cotangent of
+// the step's end state and of the saves that fell inside the step into the
+// cotangent of y_m and of the parameters.  Rejected steps leave no trace in the
+// solution and none here; step sizes are constants of the discrete map, so the
+// gradient is the exact derivative of the solution the forward pass produced.
+//
+// Reverse-mode pieces of the traced right-hand side come from the generated
+// problem source: mdx_vjp (J^T r, f_p^T r at a stage point), mdx_hvp
+// (grad (r . J(y, p) k), the dependence of the iteration matrix on y and p) and
+// mdx_ft_vjp (grad (d . df/dt)).  The discrete adjoint has no counterpart in
+// the reference, whose gradients come from forward sensitivities
+// (modax/_sensitivity.py:331-413); for a fixed step sequence the two are the
+// transposes of one linear map, which is what the tests check.
+#pragma once
+
+namespace mdx {
+namespace adjoint {
+
+__device__ __forceinline__ const double* ckpt_record(const MdxGradArgs& a, int m, int traj) {
+  return a.ckpt + ((size_t)m * (size_t)a.n_traj + (size_t)traj) * (MDX_NV + 2);
+}
+
+// The highest save index whose time a step ending at `t_end` reaches, searching
+// down from `hi` (the forward pass's save rule, mdx_common.cuh::save_reached).
+__device__ __forceinline__ int last_save_reached(const double* times, int hi, double t_end) {
+  int s = hi;
+  while (s > 0 && !save_reached(times[s], t_end)) --s;
+  return s;
+}
+
+__device__ __forceinline__ const double* grad_row(const MdxGradArgs& a, int traj, int s) {
+  return a.grad_hist + ((size_t)traj * (size_t)a.n_save + (size_t)s) * MDX_NV;
+}
+
+}  // namespace adjoint
+}  // namespace mdx
+
+#if defined(MDX_ADJOINT_RODAS5P)
+namespace mdx {
+namespace adjoint {
+using namespace mdx::rodas5p;
+
+// Reverse of one accepted Rodas5P step.  On entry ybar holds the cotangent of
+// the step's end state; on exit the cotangent of its start state; pbar
+// accumulates.  Saves s_lo < s <= s_hi fell inside this step.
+__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
+                                             const double (&y)[MDX_NV], const double* p,
+                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
+                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
+  typedef MDX_LU_T T;
+  const double inv_dt = 1.0 / h;
+  const double t_end = t + h;
+  const double dtgamma_inv = 1.0 / (h * GAMMA);
+  T lu[MDX_LU_SIZE];
+  int ipiv[MDX_IPIV];
+  double dT[MDX_NV];
+  mdx_neg_jac(y, t, p, lu, dT);
+#pragma unroll
+  for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (T)dtgamma_inv;
+  mdx_factorize(lu, ipiv);
+
+  // Recompute the stages exactly as the forward step did.
+  T k[8][MDX_NV];
+  double u[MDX_NV], work[MDX_NV];
+  T rhs[MDX_NV];
+  double us[8][MDX_NV];  // the point each stage's f was evaluated at
+  const double tstage[8] = {t, t + coef_ct(0) * h, t + coef_ct(1) * h, t + coef_ct(2) * h,
+                            t + coef_ct(3) * h, t_end, t_end, t_end};
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    if (s == 0) {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) u[j] = y[j];
+    } else if (s <= 5) {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) {
+        double acc = coef_a(s - 1, 0) * (double)k[0][j];
+#pragma unroll
+        for (int m = 1; m < s; ++m) acc += coef_a(s - 1, m) * (double)k[m][j];
+        u[j] = y[j] + acc;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) u[j] += (double)k[s - 1][j];
+    }
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) us[s][j] = u[j];
+    mdx_rhs(u, tstage[s], p, work);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      double value;
+      if (s == 0) {
+        value = work[j] + h * coef_d(0) * dT[j];
+      } else {
+        double acc = coef_c(s, 0) * (double)k[0][j];
+#pragma unroll
+        for (int m = 1; m < s; ++m) acc += coef_c(s, m) * (double)k[m][j];
+        if (coef_d(s) != 0.0) value = work[j] + h * coef_d(s) * dT[j] + acc * inv_dt;
+        else value = work[j] + acc * inv_dt;
+      }
+      rhs[j] = (T)value;
+    }
+    mdx_solve(lu, ipiv, rhs);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) k[s][j] = rhs[j];
+  }
+
+  // Cotangents of the stages, starting from the end state and the saves.
+  double kbar[8][MDX_NV];
+  double ynew_bar[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ynew_bar[j] = ybar[j];
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) kbar[s][j] = 0.0;
+  double ystart_bar[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ystart_bar[j] = 0.0;
+  for (int sv = s_lo + 1; sv <= s_hi; ++sv) {
+    const double theta = (a.times[sv] - t) / h;
+    const double theta1 = 1.0 - theta;
+    const double* g = grad_row(a, traj, sv);
+    const double w1 = theta * theta1, w2 = theta * theta * theta1, w3 = theta * theta * theta * theta1;
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      const double gj = g[j];
+      ystart_bar[j] += theta1 * gj;
+      ynew_bar[j] += theta * gj;
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        kbar[m][j] += (coef_h(0, m) * w1 + coef_h(1, m) * w2 + coef_h(2, m) * w3) * gj;
+    }
+  }
+  // y_new = y + sum_{m<=4} A[4][m] k_m + k5 + k6 + k7
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) {
+    ystart_bar[j] += ynew_bar[j];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) kbar[m][j] += coef_a(4, m) * ynew_bar[j];
+    kbar[5][j] += ynew_bar[j];
+    kbar[6][j] += ynew_bar[j];
+    kbar[7][j] += ynew_bar[j];
+  }
+
+  double dTbar[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) dTbar[j] = 0.0;
+  double uchain[MDX_NV];  // cotangent flowing down the u5 -> u6 -> u7 chain
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) uchain[j] = 0.0;
+
+#pragma unroll
+  for (int s = 7; s >= 0; --s) {
+    T rb_t[MDX_NV];
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) rb_t[j] = (T)kbar[s][j];
+    mdx_solve_t(lu, ipiv, rb_t);
+    double rbar[MDX_NV];
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) rbar[j] = (double)rb_t[j];
+    // k_s = W^-1 r_s with W = I/(h gamma) - J(y, p): J-bar = rbar k_s^T.
+    double kd[MDX_NV];
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) kd[j] = (double)k[s][j];
+    mdx_hvp(y, t, p, kd, rbar, ystart_bar, pbar);
+    // r_s = f(u_s) + h d_s dT + (sum_m C[s][m] k_m) / h
+    if (coef_d(s) != 0.0) {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) dTbar[j] += h * coef_d(s) * rbar[j];
+    }
+#pragma unroll
+    for (int m = 0; m < s; ++m)
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) kbar[m][j] += coef_c(s, m) * inv_dt * rbar[j];
+    double ubar[MDX_NV];
+    mdx_vjp(us[s], tstage[s], p, rbar, ubar, pbar);
+    if (s >= 5) {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) ubar[j] += uchain[j];
+    }
+    if (s == 7 || s == 6) {
+      // u_s = u_{s-1} + k_{s-1}
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) {
+        uchain[j] = ubar[j];
+        kbar[s - 1][j] += ubar[j];
+      }
+    } else if (s >= 1) {
+      // u_s = y + sum_{m<s} A[s-1][m] k_m
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) {
+        ystart_bar[j] += ubar[j];
+#pragma unroll
+        for (int m = 0; m < s; ++m) kbar[m][j] += coef_a(s - 1, m) * ubar[j];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) ystart_bar[j] += ubar[j];
+    }
+  }
+  mdx_ft_vjp(y, t, p, dTbar, ystart_bar, pbar);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ybar[j] = ystart_bar[j];
+}
+
+}  // namespace adjoint
+}  // namespace mdx
+#endif
+
+#if defined(MDX_ADJOINT_TSIT5)
+namespace mdx {
+namespace adjoint {
+using namespace mdx::tsit5;
+
+__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
+                                             const double (&y)[MDX_NV], const double* p,
+                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
+                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
+  // Tsit5 rows: u_s = y + h * sum_{m<s} a[s][m] k_m, k_s = f(u_s, t + c_s h);
+  // y_new = u_7 (the B row), k_7 = f(y_new, t + h).
+  const double arow[7][6] = {
+      {0, 0, 0, 0, 0, 0},
+      {A21, 0, 0, 0, 0, 0},
+      {A31, A32, 0, 0, 0, 0},
+      {A41, A42, A43, 0, 0, 0},
+      {A51, A52, A53, A54, 0, 0},
+      {A61, A62, A63, A64, A65, 0},
+      {B1, B2, B3, B4, B5, B6},
+  };
+  const double cs[7] = {0.0, C2, C3, C4, C5, 1.0, 1.0};
+  double k[7][MDX_NV], us[7][MDX_NV];
+#pragma unroll
+  for (int s = 0; s < 7; ++s) {
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      if (s == 0) {
+        us[s][j] = y[j];
+      } else {
+        double acc = arow[s][0] * k[0][j];
+#pragma unroll
+        for (int m = 1; m < s; ++m) acc += arow[s][m] * k[m][j];
+        us[s][j] = y[j] + h * acc;
+      }
+    }
+    mdx_rhs(us[s], t + cs[s] * h, p, k[s]);
+  }
+  // k[6] is f(y_new, t + h); the end state is us[6].
+  double kbar[7][MDX_NV], ystart_bar[MDX_NV], ynew_bar[MDX_NV];
+#pragma unroll
+  for (int s = 0; s < 7; ++s)
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) kbar[s][j] = 0.0;
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) {
+    ystart_bar[j] = 0.0;
+    ynew_bar[j] = ybar[j];
+  }
+  for (int sv = s_lo + 1; sv <= s_hi; ++sv) {
+    const double theta = (a.times[sv] - t) / h;
+    double b[7];
+    dense_weights(theta, b);
+    const double* g = grad_row(a, traj, sv);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      ystart_bar[j] += g[j];
+#pragma unroll
+      for (int m = 0; m < 7; ++m) kbar[m][j] += h * b[m] * g[j];
+    }
+  }
+  // k7 = f(y_new): its cotangent flows into y_new first.
+  double ub[MDX_NV];
+  mdx_vjp(us[6], t + h, p, kbar[6], ub, pbar);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ynew_bar[j] += ub[j];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) {
+    ystart_bar[j] += ynew_bar[j];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) kbar[m][j] += h * arow[6][m] * ynew_bar[j];
+  }
+#pragma unroll
+  for (int s = 5; s >= 0; --s) {
+    mdx_vjp(us[s], t + cs[s] * h, p, kbar[s], ub, pbar);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      ystart_bar[j] += ub[j];
+#pragma unroll
+      for (int m = 0; m < s; ++m) kbar[m][j] += h * arow[s][m] * ub[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ybar[j] = ystart_bar[j];
+}
+
+}  // namespace adjoint
+}  // namespace mdx
+#endif
+
+// The reverse pass: saves after the last accepted step hold the final state
+// (Rodas5P's frozen saves), save 0 is y0 itself.
+extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
+mdx_grad_reverse(const MdxGradArgs a) {
+  const int traj = blockIdx.x * blockDim.x + threadIdx.x;
+  if (traj >= a.n_traj) return;
+  double p[MDX_NP > 0 ? MDX_NP : 1];
+#pragma unroll
+  for (int k = 0; k < MDX_NP; ++k) p[k] = a.params[(size_t)traj * MDX_NP + k];
+  double pbar[MDX_NP > 0 ? MDX_NP : 1];
+#pragma unroll
+  for (int k = 0; k < MDX_NP; ++k) pbar[k] = 0.0;
+  double ybar[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ybar[j] = 0.0;
+  const int n_steps = a.ckpt_count[traj];
+  int status = 0;
+  if (n_steps > a.ckpt_capacity) status |= MDX_STATUS_CKPT_OVERFLOW;
+  const int steps = n_steps < a.ckpt_capacity ? n_steps : (int)a.ckpt_capacity;
+  int s_hi = a.n_save - 1;
+  if (steps > 0) {
+    const double* rec = mdx::adjoint::ckpt_record(a, steps - 1, traj);
+    s_hi = mdx::adjoint::last_save_reached(a.times, a.n_save - 1, rec[0] + rec[1]);
+  } else {
+    s_hi = 0;
+  }
+  // Frozen saves past the last accepted step are the final state.
+  for (int sv = s_hi + 1; sv < a.n_save; ++sv) {
+    const double* g = mdx::adjoint::grad_row(a, traj, sv);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+  }
+  for (int m = steps - 1; m >= 0; --m) {
+    const double* rec = mdx::adjoint::ckpt_record(a, m, traj);
+    const double t = rec[0], h = rec[1];
+    double y[MDX_NV];
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) y[j] = rec[2 + j];
+    const int s_lo = m == 0 ? 0 : mdx::adjoint::last_save_reached(a.times, s_hi, t);
+    mdx::adjoint::reverse_step(a, traj, t, h, y, p, s_lo, s_hi, ybar, pbar);
+    s_hi = s_lo;
+  }
+  const double* g0 = mdx::adjoint::grad_row(a, traj, 0);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) a.grad_y0[(size_t)traj * MDX_NV + j] = ybar[j] + g0[j];
+#pragma unroll
+  for (int k = 0; k < MDX_NP; ++k) a.grad_params[(size_t)traj * MDX_NP + k] = pbar[k];
+  if (a.status) a.status[traj] = status;
+}

@@ -716,4 +716,11 @@ int oracle_jvp(const SystemDesc* s, const double* y, double t, const double* p, 
   return 0;
 }
 
+int oracle_jvp2(const SystemDesc* s, const double* y, double t, const double* p, const double* uy,
+                double ut, const double* up, const double* vy, double vt, const double* vp,
+                double* out) {
+  jvp2(*s, y, t, p, uy, ut, up, vy, vt, vp, out);
+  return 0;
+}
+
 }  // extern "C"

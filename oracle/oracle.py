@@ -116,6 +116,9 @@ def lib():
         L.oracle_eval.argtypes = [ctypes.POINTER(_SystemDesc)] + [ctypes.c_void_p, ctypes.c_double,
                                                                   ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_jvp2.argtypes = [ctypes.POINTER(_SystemDesc), ctypes.c_void_p, ctypes.c_double,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_jvp.argtypes = [ctypes.POINTER(_SystemDesc), ctypes.c_void_p, ctypes.c_double,
                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
                                  ctypes.c_void_p]
@@ -469,5 +472,17 @@ def jvp(system: System, y, t, p, vy, vt=0.0, vp=None):
     out = np.empty(system.n)
     desc, keep = system._desc()
     lib().oracle_jvp(ctypes.byref(desc), _ptr(y), float(t), _ptr(p), _ptr(vy), float(vt), _ptr(vp), _ptr(out))
+    del keep
+    return out
+
+
+def jvp2(system: System, y, t, p, uy, ut, up, vy, vt, vp):
+    """Second directional derivative D^2 f(y, t, p)[u, v] of the system's right-hand side."""
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (y, p, uy, up, vy, vp)]
+    y, p, uy, up, vy, vp = arr
+    out = np.empty(system.n)
+    desc, keep = system._desc()
+    lib().oracle_jvp2(ctypes.byref(desc), _ptr(y), float(t), _ptr(p), _ptr(uy), float(ut), _ptr(up),
+                      _ptr(vy), float(vt), _ptr(vp), _ptr(out))
     del keep
     return out

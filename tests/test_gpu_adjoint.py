@@ -1,0 +1,139 @@
+"""The discrete adjoint (torch autograd over ``mdx_grad``) against independent gradients.
+
+* closed-form sensitivities of the linear cascade (tests/test_sensitivity.py:41-83
+  in the reference),
+* the oracle's forward sensitivities on the same step sequence
+  (``sens_error_control=False`` semantics, modax/_sensitivity.py:274-292): the
+  discrete adjoint and the discrete forward sensitivities are transposes of one
+  linear map, so they agree to rounding,
+* central differences of the GPU solve itself (step sizes move with the
+  perturbation, so the agreement is to the solver tolerance).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from menodax_b200 import rodas5P, systems, tsit5
+
+pytestmark = pytest.mark.gpu
+
+A, B = 0.7, 1.3
+Y0 = np.array([2.0, 0.5])
+T_SPAN = np.linspace(0.0, 2.0, 5)
+
+
+def cascade_exact_sens(t, y0, p):
+    a, b = p
+    c0, c1 = y0
+    k = a / (b - a)
+    dk_da = b / (b - a) ** 2
+    dk_db = -a / (b - a) ** 2
+    ea, eb = np.exp(-a * t), np.exp(-b * t)
+    d_da = np.stack([-t * c0 * ea, c0 * (dk_da * (ea - eb) - k * t * ea)], axis=-1)
+    d_db = np.stack([np.zeros_like(t), c0 * dk_db * (ea - eb) - t * (c1 - k * c0) * eb], axis=-1)
+    d_dc0 = np.stack([ea, k * (ea - eb)], axis=-1)
+    d_dc1 = np.stack([np.zeros_like(t), eb], axis=-1)
+    return np.stack([d_dc0, d_dc1], axis=-1), np.stack([d_da, d_db], axis=-1)
+
+
+def _grads(solve, fn, y0, t_span, params, w, **kw):
+    y0_t = torch.tensor(y0, dtype=torch.float64, device="cuda", requires_grad=True)
+    p_t = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
+    hist = solve(fn, y0_t, t_span, p_t, **kw)
+    loss = (hist * torch.as_tensor(w, device="cuda")).sum()
+    loss.backward()
+    return hist.detach().cpu().numpy(), y0_t.grad.cpu().numpy(), p_t.grad.cpu().numpy()
+
+
+@pytest.mark.parametrize("solve,kw", [
+    (rodas5P.solve, dict(lu_precision="fp64")),
+    (tsit5.solve, {}),
+])
+def test_cascade_gradient_matches_closed_form(solve, kw):
+    n = 4
+    y0 = np.broadcast_to(Y0, (n, 2)).copy()
+    p = np.broadcast_to([A, B], (n, 2)).copy()
+    rng = np.random.default_rng(0)
+    w = rng.normal(size=(n, len(T_SPAN), 2))
+    _, gy, gp = _grads(solve, systems.cascade, y0, T_SPAN, p, w, rtol=1e-10, atol=1e-12, **kw)
+    sy, sp = cascade_exact_sens(T_SPAN, Y0, (A, B))
+    ey = np.einsum("nsj,sjk->nk", w, sy)
+    ep = np.einsum("nsj,sjk->nk", w, sp)
+    np.testing.assert_allclose(gy, ey, rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(gp, ep, rtol=1e-6, atol=1e-9)
+
+
+def _sens_grads(oracle, solver, system, y0, t_span, params, w, **kw):
+    n_vars = system.n
+    hist, *_ = oracle.solve(solver, system, y0, t_span, params,
+                            sens=(True, list(range(system.np)), False), **kw)
+    n_sens = n_vars + system.np
+    sens = hist[:, :, n_vars:].reshape(hist.shape[0], hist.shape[1], n_sens, n_vars)
+    g = np.einsum("nsj,nskj->nk", w, sens)
+    return hist[:, :, :n_vars], g[:, :n_vars], g[:, n_vars:]
+
+
+def test_robertson_adjoint_matches_oracle_forward_sensitivities(oracle):
+    cfg = systems.robertson_config(size=64)
+    rng = np.random.default_rng(1)
+    w = rng.normal(size=(64, len(cfg["t_span"]), 3))
+    h, gy, gp = _grads(rodas5P.solve, cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], w,
+                       rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    oh, oy, op = _sens_grads(oracle, "rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"],
+                             cfg["params"], w, rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    np.testing.assert_allclose(h, oh, rtol=1e-9, atol=1e-15)
+    scale_y = np.abs(oy).max(axis=1, keepdims=True) + 1e-300
+    scale_p = np.abs(op).max(axis=1, keepdims=True) + 1e-300
+    assert (np.abs(gy - oy) / scale_y).max() < 1e-7
+    assert (np.abs(gp - op) / scale_p).max() < 1e-7
+
+
+def test_lorenz_tsit5_adjoint_matches_oracle_forward_sensitivities(oracle):
+    cfg = systems.lorenz_config(size=64)
+    rng = np.random.default_rng(2)
+    w = rng.normal(size=(64, len(cfg["t_span"]), 3))
+    h, gy, gp = _grads(tsit5.solve, cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], w,
+                       rtol=cfg["rtol"], atol=cfg["atol"])
+    oh, oy, op = _sens_grads(oracle, "tsit5", oracle.System.lorenz(), cfg["y0"], cfg["t_span"],
+                             cfg["params"], w, rtol=cfg["rtol"], atol=cfg["atol"])
+    np.testing.assert_allclose(h, oh, rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(gy, oy, rtol=1e-7, atol=1e-9 * np.abs(oy).max())
+    np.testing.assert_allclose(gp, op, rtol=1e-7, atol=1e-9 * np.abs(op).max())
+
+
+def test_forced_decay_gradient_uses_df_dt(oracle):
+    """Non-autonomous: the df/dt term's own derivative reaches the gradient."""
+    t_span = np.linspace(0.0, 1.0, 11)
+    y0 = np.zeros((3, 1))
+    p = np.array([[10.0, 5.0], [8.0, 3.0], [12.0, 1.0]])
+    w = np.ones((3, 11, 1))
+    _, gy, gp = _grads(rodas5P.solve, systems.forced_decay, y0, t_span, p, w, rtol=1e-10,
+                       atol=1e-12, first_step=1e-4, lu_precision="fp64")
+    _, oy, op = _sens_grads(oracle, "rodas5P", oracle.System.forced(), y0, t_span, p, w,
+                            rtol=1e-10, atol=1e-12, first_step=1e-4, lu_precision="fp64")
+    np.testing.assert_allclose(gp, op, rtol=1e-7)
+    np.testing.assert_allclose(gy, oy, rtol=1e-7, atol=1e-12)
+
+
+def test_vdp_adjoint_against_central_differences():
+    cfg = systems.vdp_gradient_config(1, size=8)
+    fn = cfg["ode_fn"]
+    t_span = np.linspace(0.0, 10.0, 6)
+    y0, p = cfg["y0"], cfg["params"] * 0 + 5.0
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=(8, len(t_span), 2))
+    kw = dict(rtol=1e-10, atol=1e-12, lu_precision="fp64")
+    _, gy, gp = _grads(rodas5P.solve, fn, y0, t_span, p, w, **kw)
+
+    def loss(y0_, p_):
+        return (rodas5P.solve(fn, y0_, t_span, p_, **kw) * w).sum(axis=(1, 2))
+
+    eps = 1e-6
+    fd = (loss(y0, p * (1 + eps)) - loss(y0, p * (1 - eps))) / (2 * eps * p[:, 0])
+    np.testing.assert_allclose(gp[:, 0], fd, rtol=1e-4)
+    for j in range(2):
+        dy = np.zeros_like(y0)
+        dy[:, j] = eps
+        fd = (loss(y0 + dy, p) - loss(y0 - dy, p)) / (2 * eps)
+        np.testing.assert_allclose(gy[:, j], fd, rtol=1e-4, atol=1e-6)

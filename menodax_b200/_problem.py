@@ -42,6 +42,7 @@ class KernelOptions:
     min_blocks: int = 1
     sparsity: tuple | None = None
     ordering: str = "amd"
+    sparse_code: str = "auto"
     tf_index: int = -1
     max_registers: int | None = None
     save_history: bool = True
@@ -144,7 +145,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
             lu_size = structure.size
             parts.append(f"#define MDX_LU_SIZE {lu_size}")
             parts.append("#define MDX_IPIV 1")
-            parts.append(emit_sparse_lu(sparse.layout, sparse.ops))
+            parts.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code))
             diag = structure.diagonal
             cases = " ".join(f"case {d}: return {int(s)};" for d, s in enumerate(diag))
             parts.append(

@@ -245,13 +245,17 @@ def _c_array(name: str, values) -> str:
     return f"__constant__ int {name}[{max(1, len(values))}] = {{{body}}};"
 
 
-def emit_cuda(layout: SparseLULayout, ops) -> str:
+def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto") -> str:
     """``mdx_sparse_factorize`` / ``mdx_sparse_solve`` / ``mdx_sparse_solve_t`` for one layout.
 
     ``T`` is the LU element type.  Multipliers and updates run in ``T`` and the
     reciprocal pivot is formed in double, as ``modax`` does (numba's typing of
-    ``1.0 / lu[pivot]``, ``modax/_sparse_direct.py:520, 545``).
+    ``1.0 / lu[pivot]``, ``modax/_sparse_direct.py:520, 545``).  ``mode`` is
+    ``"auto"`` (straight-line below the size thresholds), ``"unrolled"`` or
+    ``"tables"``; the two forms perform the same operations in the same order.
     """
+    if mode not in ("auto", "unrolled", "tables"):
+        raise ValueError(f"sparse code mode must be 'auto', 'unrolled' or 'tables'; got {mode!r}")
     n = layout.n_vars
     row_ptr, diag_ptr = layout.row_ptr, layout.diag_ptr
     origin, col_origin = layout.row_origin, layout.col_origin
@@ -260,7 +264,9 @@ def emit_cuda(layout: SparseLULayout, ops) -> str:
     _, updates, substitutions = layout.flop_counts()
     out = []
 
-    if destination.size <= MAX_UNROLLED_UPDATES:
+    unroll_factor = mode == "unrolled" or (mode == "auto" and destination.size <= MAX_UNROLLED_UPDATES)
+    unroll_solve = mode == "unrolled" or (mode == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS)
+    if unroll_factor:
         lines = []
         for i in range(n):
             for p in range(int(row_ptr[i]), int(diag_ptr[i])):
@@ -297,7 +303,7 @@ def emit_cuda(layout: SparseLULayout, ops) -> str:
             "  }\n}"
         )
 
-    if substitutions <= MAX_UNROLLED_SUBSTITUTIONS:
+    if unroll_solve:
         fwd, back, tfwd, tback = [], [], [], []
         for i in range(n):
             row = int(origin[i])

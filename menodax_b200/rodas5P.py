@@ -62,6 +62,7 @@ def solve(
     hook_size: int = 0,
     save_history: bool = True,
     launch: str = "auto",
+    sparse_code: str = "auto",
 ):
     """Rodas5P ensemble solve of ``y' = ode_fn(y, t, p)`` on one GPU.
 
@@ -101,6 +102,7 @@ def solve(
         threads_per_block=_block_size(tpb),
         sparsity=sparsity,
         ordering=ordering,
+        sparse_code=sparse_code,
         tf_index=-1 if tf_index is None else int(tf_index),
         max_registers=max_registers,
         save_history=bool(save_history),

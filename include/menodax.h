@@ -65,7 +65,7 @@ typedef struct mdx_plan_desc {
   int n_params;
   int threads_per_block;  /* the block size the module was compiled for */
   int flags;              /* MDX_PLAN_* */
-  int reserved;
+  int ckpt_stride;        /* MDX_PLAN_CHECKPOINT: steps per recorded start state (>= 1) */
   const void* cubin;
   size_t cubin_size;
 } mdx_plan_desc;
@@ -95,7 +95,7 @@ typedef struct mdx_solve_desc {
   const int* order;       /* persistent: optional trajectory visiting order, or NULL */
   void* workspace;        /* persistent: >= mdx_workspace_size() bytes */
   size_t workspace_bytes;
-  double* ckpt;           /* MDX_PLAN_CHECKPOINT: (ckpt_capacity, n_traj, n_vars + 2) */
+  double* ckpt;           /* MDX_PLAN_CHECKPOINT: mdx_checkpoint_size() bytes */
   int* ckpt_count;        /* MDX_PLAN_CHECKPOINT: (n_traj,) */
   long long ckpt_capacity;
   int grid_blocks;        /* persistent: 0 = occupancy-sized */
@@ -134,6 +134,11 @@ int mdx_plan_destroy(mdx_plan* plan);
 
 /* Bytes of `workspace` a solve in `mode` needs (0 for MDX_LAUNCH_PLAIN). */
 int mdx_workspace_size(const mdx_plan* plan, int mode, int n_traj, size_t* bytes);
+
+/* Bytes of the checkpoint buffer a MDX_PLAN_CHECKPOINT solve of n_traj
+ * trajectories needs to record up to `capacity` accepted steps each: every step
+ * size, plus the start (t, y) of every ckpt_stride-th step. */
+int mdx_checkpoint_size(const mdx_plan* plan, int n_traj, long long capacity, size_t* bytes);
 
 /* Resident blocks per SM for the plan's kernel in `mode`, and the SM count of
  * the current device (loads the module on first use). */

@@ -38,7 +38,7 @@ MDX_STATUS_CKPT_OVERFLOW = 4
 EXPORTED = (
     "mdx_compile", "mdx_free", "mdx_plan_create", "mdx_plan_destroy", "mdx_workspace_size",
     "mdx_occupancy", "mdx_solve", "mdx_grad", "mdx_last_error", "mdx_version",
-    "mdx_measure_fma_peak", "mdx_solve_persistent_noalloc",
+    "mdx_measure_fma_peak", "mdx_solve_persistent_noalloc", "mdx_checkpoint_size",
 )
 
 
@@ -50,7 +50,7 @@ class PlanDesc(ctypes.Structure):
     _fields_ = [
         ("struct_size", ctypes.c_int), ("solver", ctypes.c_int), ("n_vars", ctypes.c_int),
         ("n_system", ctypes.c_int), ("n_params", ctypes.c_int),
-        ("threads_per_block", ctypes.c_int), ("flags", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("threads_per_block", ctypes.c_int), ("flags", ctypes.c_int), ("ckpt_stride", ctypes.c_int),
         ("cubin", ctypes.c_void_p), ("cubin_size", ctypes.c_size_t),
     ]
 
@@ -131,6 +131,7 @@ def lib():
         L.mdx_plan_create.argtypes = [ctypes.POINTER(PlanDesc), ctypes.POINTER(ctypes.c_void_p)]
         L.mdx_plan_destroy.argtypes = [ctypes.c_void_p]
         L.mdx_workspace_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+        L.mdx_checkpoint_size.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.POINTER(ctypes.c_size_t)]
         L.mdx_occupancy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.mdx_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(SolveDesc), ctypes.c_void_p]
         L.mdx_grad.argtypes = [ctypes.c_void_p, ctypes.POINTER(GradDesc), ctypes.c_void_p]
@@ -208,11 +209,11 @@ class Plan:
     """Owns one ``mdx_plan``: a compiled problem, loaded lazily per CUDA context."""
 
     def __init__(self, solver: int, n_vars: int, n_system: int, n_params: int, tpb: int,
-                 flags: int, cubin: bytes):
+                 flags: int, cubin: bytes, ckpt_stride: int = 1):
         self._cubin = ctypes.create_string_buffer(cubin, len(cubin))
         desc = PlanDesc(
             struct_size=ctypes.sizeof(PlanDesc), solver=solver, n_vars=n_vars, n_system=n_system,
-            n_params=n_params, threads_per_block=tpb, flags=flags, reserved=0,
+            n_params=n_params, threads_per_block=tpb, flags=flags, ckpt_stride=ckpt_stride,
             cubin=ctypes.cast(self._cubin, ctypes.c_void_p), cubin_size=len(cubin),
         )
         handle = ctypes.c_void_p()
@@ -235,6 +236,11 @@ class Plan:
         b, s = ctypes.c_int(), ctypes.c_int()
         check(lib().mdx_occupancy(self.handle, mode, ctypes.byref(b), ctypes.byref(s)), "mdx_occupancy")
         return b.value, s.value
+
+    def checkpoint_size(self, n_traj: int, capacity: int) -> int:
+        out = ctypes.c_size_t()
+        check(lib().mdx_checkpoint_size(self.handle, n_traj, capacity, ctypes.byref(out)), "mdx_checkpoint_size")
+        return out.value
 
     def workspace_size(self, mode: int, n_traj: int) -> int:
         out = ctypes.c_size_t()

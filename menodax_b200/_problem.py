@@ -50,6 +50,7 @@ class KernelOptions:
     # Forward sensitivities: (n_y0_dirs, param columns, error_control), or None.
     sens: tuple | None = None
     checkpoint: bool = False
+    ckpt_stride: int = 1
     adjoint: bool = False
 
 
@@ -111,6 +112,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         f"#define MDX_WEIGHTS_RUNTIME {1 if options.runtime_weights else 0}",
         f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
         f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
+        f"#define MDX_CKPT_SEG {int(options.ckpt_stride)}",
         f"#define MDX_TPB {int(options.threads_per_block)}",
         f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
         '#include "mdx_common.cuh"',
@@ -201,7 +203,8 @@ def get_problem(ode_fn, n_vars: int, n_params: int, options: KernelOptions) -> P
         _native.MDX_PLAN_ADJOINT if options.adjoint else 0
     )
     solver = _native.MDX_SOLVER_TSIT5 if options.solver == "tsit5" else _native.MDX_SOLVER_RODAS5P
-    plan = _native.Plan(solver, n_vars, meta["n_system"], n_params, options.threads_per_block, flags, cubin)
+    plan = _native.Plan(solver, n_vars, meta["n_system"], n_params, options.threads_per_block, flags, cubin,
+                        ckpt_stride=int(options.ckpt_stride))
     prob = Problem(
         plan=plan, source=source, n_vars=n_vars, n_system=meta["n_system"], n_params=n_params,
         n_error=meta["n_error"], options=options, lu_size=meta["lu_size"], sparse=meta["sparse"],

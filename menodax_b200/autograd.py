@@ -23,8 +23,32 @@ from menodax_b200._ensemble import initial_step, launch, pick_device, solver_sta
 from menodax_b200._problem import get_problem
 
 # Checkpoint capacity (accepted steps per trajectory) last seen per problem, so a
-# repeated gradient call allocates once and runs the forward pass once.
+# repeated gradient call sizes its buffer without a counting pass.
 _capacity_hint: dict = {}
+
+# Steps per recorded start state.  One record per step costs (n + 2) doubles a
+# step; a stride K costs 1 + (n + 1) / K and one forward replay per step in the
+# reverse pass.  The smallest stride whose buffer fits the memory budget wins.
+CKPT_STRIDES = (1, 8, 32)
+MEMORY_FRACTION = 0.6
+
+
+def checkpoint_bytes(n_traj, n_vars, capacity, stride):
+    segments = -(-capacity // stride)
+    return 8 * (capacity * n_traj + segments * n_traj * (n_vars + 1))
+
+
+def choose_stride(n_traj, n_vars, capacity, device):
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = MEMORY_FRACTION * free
+    for stride in CKPT_STRIDES:
+        if checkpoint_bytes(n_traj, n_vars, capacity, stride) <= budget:
+            return stride
+    need = checkpoint_bytes(n_traj, n_vars, capacity, CKPT_STRIDES[-1])
+    raise MemoryError(
+        f"the checkpoints of {n_traj} trajectories x {capacity} accepted steps need "
+        f"{need / 2**30:.1f} GiB even at stride {CKPT_STRIDES[-1]}; solve fewer trajectories per call"
+    )
 
 
 def needs_grad(*xs) -> bool:
@@ -39,20 +63,24 @@ def _as_double(x, device):
 
 class _EnsembleSolve(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, y0, params, times, problem, dt0, rtol, atol, max_steps, key):
+    def forward(ctx, y0, params, times, problems, dt0, rtol, atol, max_steps, key):
         n = y0.shape[0]
-        n_vars = problem.n_vars
         y0c = y0.detach().contiguous()
         pc = params.detach().contiguous()
-        capacity = _capacity_hint.get(key, 256)
+        kw = dict(y0=y0c, times=times, params=pc, weights=None, dt0=dt0, rtol=rtol, atol=atol,
+                  max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN)
+        capacity = _capacity_hint.get(key)
+        if capacity is None:
+            # First call for this problem: count the accepted steps with a plain solve.
+            _, counters = launch(problems["plain"], **kw)
+            capacity = max(1, int(counters[0].max().item()) if n else 1)
         while True:
-            ckpt = torch.empty((capacity, n, n_vars + 2), dtype=torch.float64, device=y0.device)
+            stride = choose_stride(n, problems["plain"].n_vars, capacity, y0.device)
+            problem = problems[stride]
+            nbytes = problem.plan.checkpoint_size(n, capacity)
+            ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
-            hist, counters = launch(
-                problem, y0=y0c, times=times, params=pc, weights=None, dt0=dt0, rtol=rtol, atol=atol,
-                max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN, ckpt=ckpt,
-                ckpt_count=ckpt_count, ckpt_capacity=capacity,
-            )
+            hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity, **kw)
             needed = int(counters[0].max().item()) if n else 0
             if needed <= capacity:
                 break
@@ -93,6 +121,20 @@ class _EnsembleSolve(torch.autograd.Function):
         return grad_y0, grad_p, None, None, None, None, None, None, None
 
 
+class _Problems:
+    """The plain problem and its checkpointing/adjoint variants, compiled on demand."""
+
+    def __init__(self, ode_fn, n_vars, n_params, options):
+        self.args = (ode_fn, n_vars, n_params)
+        self.options = options
+
+    def __getitem__(self, which):
+        if which == "plain":
+            return get_problem(*self.args, self.options)
+        opts = replace(self.options, checkpoint=True, adjoint=True, ckpt_stride=int(which))
+        return get_problem(*self.args, opts)
+
+
 def solve_with_grad(ode_fn, y0, t_span, params, options, *, rtol, atol, first_step, max_steps,
                     return_stats, error_weights):
     """Differentiable ensemble solve; returns torch tensors on the solve's device."""
@@ -115,10 +157,9 @@ def solve_with_grad(ode_fn, y0, t_span, params, options, *, rtol, atol, first_st
         times = t_span.detach().to(device=device, dtype=torch.float64).contiguous()
     else:
         times = torch.as_tensor(t_span, dtype=torch.float64, device=device).contiguous()
-    opts = replace(options, checkpoint=True, adjoint=True, runtime_weights=False)
-    problem = get_problem(ode_fn, n_vars, n_params, opts)
-    key = (ode_fn, n_vars, n_params, opts, n, tuple(times.tolist()), float(rtol), float(atol))
-    hist, counters = _EnsembleSolve.apply(y0_t, p_t, times, problem, initial_step(first_step), rtol,
+    problems = _Problems(ode_fn, n_vars, n_params, replace(options, runtime_weights=False))
+    key = (ode_fn, n_vars, n_params, options, n, tuple(times.tolist()), float(rtol), float(atol))
+    hist, counters = _EnsembleSolve.apply(y0_t, p_t, times, problems, initial_step(first_step), rtol,
                                           atol, max_steps, key)
     if return_stats:
         return hist, solver_stats(counters[0], counters[1], counters[2])

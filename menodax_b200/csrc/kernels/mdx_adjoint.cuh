@@ -1,11 +1,13 @@
 // Discrete adjoint of a checkpointed ensemble solve, one trajectory per thread.
 //
-// The forward solve (MDX_CHECKPOINT) records, for every accepted step m, the
-// step state (t_m, h_m, y_m).  This kernel walks the steps backwards: it
-// recomputes step m from its state -- Jacobian, df/dt, LU and the eight stages
-// (Rodas5P) or the seven stages (Tsit5) -- then back-propagates the cotangent of
-// the step's end state and of the saves that fell inside the step into the
-// cotangent of y_m and of the parameters.  Rejected steps leave no trace in the
+// The forward solve (MDX_CHECKPOINT) records every accepted step's size h_m and,
+// every MDX_CKPT_SEG steps, the step's start (t_m, y_m).  This kernel walks the
+// steps backwards a segment at a time: it replays the segment forward from its
+// recorded start to recover each step's start state, then recomputes step m --
+// Jacobian, df/dt, LU and the eight stages (Rodas5P) or the seven stages
+// (Tsit5) -- and back-propagates the cotangent of the step's end state and of
+// the saves that fell inside the step into the cotangent of y_m and of the
+// parameters.  Rejected steps leave no trace in the
 // solution and none here; step sizes are constants of the discrete map, so the
 // gradient is the exact derivative of the solution the forward pass produced.
 //
@@ -21,8 +23,13 @@
 namespace mdx {
 namespace adjoint {
 
-__device__ __forceinline__ const double* ckpt_record(const MdxGradArgs& a, int m, int traj) {
-  return a.ckpt + ((size_t)m * (size_t)a.n_traj + (size_t)traj) * (MDX_NV + 2);
+__device__ __forceinline__ double ckpt_h(const MdxGradArgs& a, int m, int traj) {
+  return a.ckpt[(size_t)m * (size_t)a.n_traj + (size_t)traj];
+}
+
+__device__ __forceinline__ const double* ckpt_seg_state(const MdxGradArgs& a, int seg, int traj) {
+  return a.ckpt + (size_t)a.ckpt_capacity * (size_t)a.n_traj +
+         ((size_t)seg * (size_t)a.n_traj + (size_t)traj) * (size_t)(MDX_NV + 1);
 }
 
 // The highest save index whose time a step ending at `t_end` reaches, searching
@@ -45,30 +52,22 @@ namespace mdx {
 namespace adjoint {
 using namespace mdx::rodas5p;
 
-// Reverse of one accepted Rodas5P step.  On entry ybar holds the cotangent of
-// the step's end state; on exit the cotangent of its start state; pbar
-// accumulates.  Saves s_lo < s <= s_hi fell inside this step.
-__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
-                                             const double (&y)[MDX_NV], const double* p,
-                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
-                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
+// Recompute one accepted Rodas5P step from its start state exactly as the
+// forward step did: the factorised iteration matrix, the eight stages and the
+// point each stage's f was evaluated at.  The end state is us[7] + k[7].
+template <class LU, class IP, class K, class US, class DTV>
+__device__ __forceinline__ void recompute(double t, double h, const double (&y)[MDX_NV], const double* p,
+                                          LU& lu, IP& ipiv, K& k, US& us, DTV& dT) {
   typedef MDX_LU_T T;
   const double inv_dt = 1.0 / h;
   const double t_end = t + h;
   const double dtgamma_inv = 1.0 / (h * GAMMA);
-  T lu[MDX_LU_SIZE];
-  int ipiv[MDX_IPIV];
-  double dT[MDX_NV];
   mdx_neg_jac(y, t, p, lu, dT);
 #pragma unroll
   for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (T)dtgamma_inv;
   mdx_factorize(lu, ipiv);
-
-  // Recompute the stages exactly as the forward step did.
-  T k[8][MDX_NV];
   double u[MDX_NV], work[MDX_NV];
   T rhs[MDX_NV];
-  double us[8][MDX_NV];  // the point each stage's f was evaluated at
   const double tstage[8] = {t, t + coef_ct(0) * h, t + coef_ct(1) * h, t + coef_ct(2) * h,
                             t + coef_ct(3) * h, t_end, t_end, t_end};
 #pragma unroll
@@ -109,6 +108,39 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 #pragma unroll
     for (int j = 0; j < MDX_NV; ++j) k[s][j] = rhs[j];
   }
+}
+
+// The end state of one accepted step, for replaying a segment forward.
+__device__ __forceinline__ void replay_step(double t, double h, const double (&y)[MDX_NV], const double* p,
+                                            double (&y_next)[MDX_NV]) {
+  MDX_LU_T lu[MDX_LU_SIZE];
+  int ipiv[MDX_IPIV];
+  MDX_LU_T k[8][MDX_NV];
+  double us[8][MDX_NV];
+  double dT[MDX_NV];
+  recompute(t, h, y, p, lu, ipiv, k, us, dT);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) y_next[j] = us[7][j] + (double)k[7][j];
+}
+
+// Reverse of one accepted Rodas5P step.  On entry ybar holds the cotangent of
+// the step's end state; on exit the cotangent of its start state; pbar
+// accumulates.  Saves s_lo < s <= s_hi fell inside this step.
+__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
+                                             const double (&y)[MDX_NV], const double* p,
+                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
+                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
+  typedef MDX_LU_T T;
+  const double inv_dt = 1.0 / h;
+  const double t_end = t + h;
+  T lu[MDX_LU_SIZE];
+  int ipiv[MDX_IPIV];
+  T k[8][MDX_NV];
+  double us[8][MDX_NV];
+  double dT[MDX_NV];
+  recompute(t, h, y, p, lu, ipiv, k, us, dT);
+  const double tstage[8] = {t, t + coef_ct(0) * h, t + coef_ct(1) * h, t + coef_ct(2) * h,
+                            t + coef_ct(3) * h, t_end, t_end, t_end};
 
   // Cotangents of the stages, starting from the end state and the saves.
   double kbar[8][MDX_NV];
@@ -218,13 +250,10 @@ namespace mdx {
 namespace adjoint {
 using namespace mdx::tsit5;
 
-__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
-                                             const double (&y)[MDX_NV], const double* p,
-                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
-                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
-  // Tsit5 rows: u_s = y + h * sum_{m<s} a[s][m] k_m, k_s = f(u_s, t + c_s h);
-  // y_new = u_7 (the B row), k_7 = f(y_new, t + h).
-  const double arow[7][6] = {
+// Tsit5 rows: u_s = y + h * sum_{m<s} a[s][m] k_m, k_s = f(u_s, t + c_s h);
+// y_new = u_7 (the B row), k_7 = f(y_new, t + h).
+__device__ __forceinline__ double arow(int s, int m) {
+  const double r[7][6] = {
       {0, 0, 0, 0, 0, 0},
       {A21, 0, 0, 0, 0, 0},
       {A31, A32, 0, 0, 0, 0},
@@ -233,8 +262,17 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
       {A61, A62, A63, A64, A65, 0},
       {B1, B2, B3, B4, B5, B6},
   };
-  const double cs[7] = {0.0, C2, C3, C4, C5, 1.0, 1.0};
-  double k[7][MDX_NV], us[7][MDX_NV];
+  return r[s][m];
+}
+
+__device__ __forceinline__ double cstage(int s) {
+  const double c[7] = {0.0, C2, C3, C4, C5, 1.0, 1.0};
+  return c[s];
+}
+
+template <class K, class US>
+__device__ __forceinline__ void recompute(double t, double h, const double (&y)[MDX_NV], const double* p,
+                                          K& k, US& us) {
 #pragma unroll
   for (int s = 0; s < 7; ++s) {
 #pragma unroll
@@ -242,14 +280,30 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
       if (s == 0) {
         us[s][j] = y[j];
       } else {
-        double acc = arow[s][0] * k[0][j];
+        double acc = arow(s, 0) * k[0][j];
 #pragma unroll
-        for (int m = 1; m < s; ++m) acc += arow[s][m] * k[m][j];
+        for (int m = 1; m < s; ++m) acc += arow(s, m) * k[m][j];
         us[s][j] = y[j] + h * acc;
       }
     }
-    mdx_rhs(us[s], t + cs[s] * h, p, k[s]);
+    mdx_rhs(us[s], t + cstage(s) * h, p, k[s]);
   }
+}
+
+__device__ __forceinline__ void replay_step(double t, double h, const double (&y)[MDX_NV], const double* p,
+                                            double (&y_next)[MDX_NV]) {
+  double k[7][MDX_NV], us[7][MDX_NV];
+  recompute(t, h, y, p, k, us);
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) y_next[j] = us[6][j];
+}
+
+__device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, double t, double h,
+                                             const double (&y)[MDX_NV], const double* p,
+                                             int s_lo, int s_hi, double (&ybar)[MDX_NV],
+                                             double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
+  double k[7][MDX_NV], us[7][MDX_NV];
+  recompute(t, h, y, p, k, us);
   // k[6] is f(y_new, t + h); the end state is us[6].
   double kbar[7][MDX_NV], ystart_bar[MDX_NV], ynew_bar[MDX_NV];
 #pragma unroll
@@ -282,16 +336,16 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
   for (int j = 0; j < MDX_NV; ++j) {
     ystart_bar[j] += ynew_bar[j];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) kbar[m][j] += h * arow[6][m] * ynew_bar[j];
+    for (int m = 0; m < 6; ++m) kbar[m][j] += h * arow(6, m) * ynew_bar[j];
   }
 #pragma unroll
   for (int s = 5; s >= 0; --s) {
-    mdx_vjp(us[s], t + cs[s] * h, p, kbar[s], ub, pbar);
+    mdx_vjp(us[s], t + cstage(s) * h, p, kbar[s], ub, pbar);
 #pragma unroll
     for (int j = 0; j < MDX_NV; ++j) {
       ystart_bar[j] += ub[j];
 #pragma unroll
-      for (int m = 0; m < s; ++m) kbar[m][j] += h * arow[s][m] * ub[j];
+      for (int m = 0; m < s; ++m) kbar[m][j] += h * arow(s, m) * ub[j];
     }
   }
 #pragma unroll
@@ -302,8 +356,11 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 }  // namespace mdx
 #endif
 
-// The reverse pass: saves after the last accepted step hold the final state
-// (Rodas5P's frozen saves), save 0 is y0 itself.
+// The reverse pass.  Segments of MDX_CKPT_SEG accepted steps are visited last
+// to first: each is replayed forward from its recorded start state (with the
+// recorded step sizes) to recover every step's start state, then reversed step
+// by step.  Saves after the last accepted step hold the final state (Rodas5P's
+// frozen saves); save 0 is y0 itself.
 extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
 mdx_grad_reverse(const MdxGradArgs a) {
   const int traj = blockIdx.x * blockDim.x + threadIdx.x;
@@ -321,28 +378,56 @@ mdx_grad_reverse(const MdxGradArgs a) {
   int status = 0;
   if (n_steps > a.ckpt_capacity) status |= MDX_STATUS_CKPT_OVERFLOW;
   const int steps = n_steps < a.ckpt_capacity ? n_steps : (int)a.ckpt_capacity;
-  int s_hi = a.n_save - 1;
-  if (steps > 0) {
-    const double* rec = mdx::adjoint::ckpt_record(a, steps - 1, traj);
-    s_hi = mdx::adjoint::last_save_reached(a.times, a.n_save - 1, rec[0] + rec[1]);
-  } else {
-    s_hi = 0;
-  }
-  // Frozen saves past the last accepted step are the final state.
-  for (int sv = s_hi + 1; sv < a.n_save; ++sv) {
-    const double* g = mdx::adjoint::grad_row(a, traj, sv);
+  int s_hi = 0;
+  if (steps == 0) {
+    for (int sv = 1; sv < a.n_save; ++sv) {
+      const double* g = mdx::adjoint::grad_row(a, traj, sv);
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+      for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+    }
   }
-  for (int m = steps - 1; m >= 0; --m) {
-    const double* rec = mdx::adjoint::ckpt_record(a, m, traj);
-    const double t = rec[0], h = rec[1];
+  double yseg[MDX_CKPT_SEG][MDX_NV];
+  double tseg[MDX_CKPT_SEG];
+  for (int seg = (steps - 1) / MDX_CKPT_SEG; steps > 0 && seg >= 0; --seg) {
+    const int m0 = seg * MDX_CKPT_SEG;
+    const int m1 = (m0 + MDX_CKPT_SEG < steps) ? m0 + MDX_CKPT_SEG : steps;
+    const double* rec = mdx::adjoint::ckpt_seg_state(a, seg, traj);
     double y[MDX_NV];
+    double t = rec[0];
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) y[j] = rec[2 + j];
-    const int s_lo = m == 0 ? 0 : mdx::adjoint::last_save_reached(a.times, s_hi, t);
-    mdx::adjoint::reverse_step(a, traj, t, h, y, p, s_lo, s_hi, ybar, pbar);
-    s_hi = s_lo;
+    for (int j = 0; j < MDX_NV; ++j) y[j] = rec[1 + j];
+    for (int m = m0; m < m1; ++m) {
+      tseg[m - m0] = t;
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) yseg[m - m0][j] = y[j];
+      const double h = mdx::adjoint::ckpt_h(a, m, traj);
+      if (m + 1 < m1) {
+        double y_next[MDX_NV];
+        mdx::adjoint::replay_step(t, h, y, p, y_next);
+#pragma unroll
+        for (int j = 0; j < MDX_NV; ++j) y[j] = y_next[j];
+      }
+      t += h;
+    }
+    if (m1 == steps) {
+      // t is now the end time of the last accepted step: later saves are frozen.
+      s_hi = mdx::adjoint::last_save_reached(a.times, a.n_save - 1, t);
+      for (int sv = s_hi + 1; sv < a.n_save; ++sv) {
+        const double* g = mdx::adjoint::grad_row(a, traj, sv);
+#pragma unroll
+        for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+      }
+    }
+    for (int m = m1 - 1; m >= m0; --m) {
+      const double tm = tseg[m - m0];
+      const double h = mdx::adjoint::ckpt_h(a, m, traj);
+      double ym[MDX_NV];
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) ym[j] = yseg[m - m0][j];
+      const int s_lo = m == 0 ? 0 : mdx::adjoint::last_save_reached(a.times, s_hi, tm);
+      mdx::adjoint::reverse_step(a, traj, tm, h, ym, p, s_lo, s_hi, ybar, pbar);
+      s_hi = s_lo;
+    }
   }
   const double* g0 = mdx::adjoint::grad_row(a, traj, 0);
 #pragma unroll

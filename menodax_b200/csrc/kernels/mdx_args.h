@@ -28,7 +28,8 @@ typedef struct MdxSolveArgs {
   double* hook_out;        /* (N, hook_size) or NULL */
   int* work_counter;       /* persistent kernels: queue head, zeroed before launch */
   const int* order;        /* persistent kernels: optional visiting order (N,) */
-  double* ckpt;            /* adjoint forward pass: (capacity, N, n_vars + 2) step states */
+  double* ckpt;            /* adjoint forward pass: step sizes (capacity, N), then segment
+                              start states (ceil(capacity / MDX_CKPT_SEG), N, n_vars + 1) */
   int* ckpt_count;         /* adjoint forward pass: accepted steps recorded per trajectory */
   long long ckpt_capacity; /* steps per trajectory the checkpoint buffer holds */
   int n_traj;

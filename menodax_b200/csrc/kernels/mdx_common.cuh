@@ -55,4 +55,28 @@ __device__ __forceinline__ bool save_reached(double ts, double t_new) {
   return ts <= t_new + 1e-12 * pymax(1.0, fabs(ts));
 }
 
+#ifndef MDX_CKPT_SEG
+#define MDX_CKPT_SEG 1
+#endif
+
+// Checkpoint layout of a MDX_CHECKPOINT solve: every accepted step's size h at
+// ckpt[m * N + traj]; every MDX_CKPT_SEG-th step's start (t, y) as a record of
+// n_vars + 1 doubles after them, segment-major so a warp in lockstep writes
+// contiguous runs.  The reverse pass replays a segment from its start state.
+__device__ __forceinline__ double* ckpt_state(double* ckpt, long long capacity, int n_traj, int seg, int traj) {
+  return ckpt + (size_t)capacity * (size_t)n_traj +
+         ((size_t)seg * (size_t)n_traj + (size_t)traj) * (size_t)(MDX_NV + 1);
+}
+
+template <class Y>
+__device__ __forceinline__ void ckpt_write(const MdxSolveArgs& a, int traj, int m, double t, double h, const Y& y) {
+  a.ckpt[(size_t)m * (size_t)a.n_traj + (size_t)traj] = h;
+  if (m % MDX_CKPT_SEG == 0) {
+    double* rec = ckpt_state(a.ckpt, a.ckpt_capacity, a.n_traj, m / MDX_CKPT_SEG, traj);
+    rec[0] = t;
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) rec[1 + j] = y[j];
+  }
+}
+
 }  // namespace mdx

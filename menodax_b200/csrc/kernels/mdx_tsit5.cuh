@@ -149,11 +149,7 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   if (accept) {
 #if MDX_CHECKPOINT
     if (st.n_ckpt < a.ckpt_capacity) {
-      double* rec = a.ckpt + ((size_t)st.n_ckpt * (size_t)a.n_traj + (size_t)st.traj) * (MDX_NV + 2);
-      rec[0] = t;
-      rec[1] = dt_use;
-#pragma unroll
-      for (int j = 0; j < MDX_NV; ++j) rec[2 + j] = st.y[j];
+      ckpt_write(a, st.traj, st.n_ckpt, t, dt_use, st.y);
       ++st.n_ckpt;
     } else {
       st.ckpt_overflow = true;

@@ -256,6 +256,8 @@ int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
   if (desc->threads_per_block <= 0 || desc->threads_per_block % 32 != 0 || desc->threads_per_block > 1024)
     return fail(MDX_E_INVALID, "threads_per_block must be a multiple of 32 in [32, 1024]; got %d", desc->threads_per_block);
   if (!desc->cubin || desc->cubin_size == 0) return fail(MDX_E_INVALID, "mdx_plan_create: empty cubin");
+  if ((desc->flags & MDX_PLAN_CHECKPOINT) && desc->ckpt_stride < 1)
+    return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt_stride >= 1; got %d", desc->ckpt_stride);
   mdx_plan* p = new (std::nothrow) mdx_plan;
   if (!p) return fail(MDX_E_NOMEM, "out of host memory");
   p->desc = *desc;
@@ -279,6 +281,17 @@ int mdx_workspace_size(const mdx_plan* plan, int mode, int n_traj, size_t* bytes
   if (!plan || !bytes) return fail(MDX_E_INVALID, "mdx_workspace_size: null argument");
   if (n_traj < 0) return fail(MDX_E_INVALID, "n_traj must be non-negative");
   *bytes = mode == MDX_LAUNCH_PERSISTENT ? 256 : 0;
+  return MDX_OK;
+}
+
+int mdx_checkpoint_size(const mdx_plan* plan, int n_traj, long long capacity, size_t* bytes) {
+  if (!plan || !bytes) return fail(MDX_E_INVALID, "mdx_checkpoint_size: null argument");
+  if (!(plan->desc.flags & MDX_PLAN_CHECKPOINT)) return fail(MDX_E_INVALID, "the plan records no checkpoints");
+  if (n_traj < 0 || capacity < 0) return fail(MDX_E_INVALID, "n_traj and capacity must be non-negative");
+  const long long stride = plan->desc.ckpt_stride;
+  const long long segments = (capacity + stride - 1) / stride;
+  *bytes = (size_t)8 * ((size_t)capacity * (size_t)n_traj +
+                        (size_t)segments * (size_t)n_traj * (size_t)(plan->desc.n_vars + 1));
   return MDX_OK;
 }
 

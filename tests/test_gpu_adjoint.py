@@ -137,3 +137,32 @@ def test_vdp_adjoint_against_central_differences():
         dy[:, j] = eps
         fd = (loss(y0 + dy, p) - loss(y0 - dy, p)) / (2 * eps)
         np.testing.assert_allclose(gy[:, j], fd, rtol=1e-4, atol=1e-6)
+
+
+@pytest.mark.parametrize("solve,kw,which", [
+    (rodas5P.solve, dict(lu_precision="fp64"), "vdp"),
+    (tsit5.solve, {}, "lorenz"),
+])
+def test_segmented_checkpoints_give_the_same_gradient(monkeypatch, solve, kw, which):
+    """Recording a start state every 8 steps and replaying the segments gives the
+    gradient of recording every step."""
+    from menodax_b200 import autograd
+
+    if which == "vdp":
+        cfg = systems.vdp_gradient_config(1, size=32)
+        t_span = np.linspace(0.0, 50.0, 7)
+    else:
+        cfg = systems.lorenz_config(size=32)
+        t_span = cfg["t_span"]
+    n_vars = cfg["y0"].shape[1]
+    w = np.random.default_rng(4).normal(size=(32, len(t_span), n_vars))
+    out = []
+    for strides in ((1,), (8,)):
+        monkeypatch.setattr(autograd, "CKPT_STRIDES", strides)
+        autograd._capacity_hint.clear()
+        out.append(_grads(solve, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], w, rtol=1e-6,
+                          atol=1e-8, **kw))
+    (h1, gy1, gp1), (h8, gy8, gp8) = out
+    assert np.array_equal(h1, h8)
+    np.testing.assert_allclose(gy8, gy1, rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(gp8, gp1, rtol=1e-10, atol=1e-14)

@@ -40,22 +40,21 @@ def _times_tensor(t_span):
     return t
 
 
-def resolve_mode(launch_mode: str, options: KernelOptions, n: int) -> int:
+# Below this many trajectories a launch is one partial wave whatever its shape,
+# and the reference's own choice (one warp per block, one launch) is kept.
+AUTOTUNE_MIN_TRAJECTORIES = 4096
+
+
+def resolve_mode(launch_mode: str) -> int:
     if launch_mode not in LAUNCH_MODES:
         raise ValueError(f"launch must be one of {LAUNCH_MODES}; got {launch_mode!r}")
-    if launch_mode == "plain":
-        return _native.MDX_LAUNCH_PLAIN
     if launch_mode == "persistent":
-        return _native.MDX_LAUNCH_PERSISTENT
-    # Uneven step counts are what the refill kernel is for; a stiff solve whose
-    # ensemble fills more than one wave of warps gains from it.
-    if options.solver == "rodas5P" and n >= 4096:
         return _native.MDX_LAUNCH_PERSISTENT
     return _native.MDX_LAUNCH_PLAIN
 
 
 def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first_step,
-        max_steps, return_stats, error_weights, launch_mode="auto", grid_blocks=0):
+        max_steps, return_stats, error_weights, launch_mode="auto", grid_blocks=0, tune_block=True):
     torch_io = _is_torch(y0, params)
     y0_t, p_t, n, n_vars = normalize_y0_params(y0, params)
     n_params = p_t.shape[1]
@@ -68,17 +67,25 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     if int(max_steps) < 0:
         raise ValueError("max_steps must be non-negative")
     device = pick_device(y0_t, p_t)
-    problem = get_problem(ode_fn, n_vars, n_params, options)
-    mode = resolve_mode(launch_mode, options, n)
+    mode = resolve_mode(launch_mode)
     y0_d = to_device(y0_t.detach(), device)
     p_d = to_device(p_t.detach(), device)
     t_d = to_device(times, device)
     w_d = to_device(weights.detach(), device) if weights is not None else None
-    hist, counters = launch(
-        problem, y0=y0_d, times=t_d, params=p_d, weights=w_d, dt0=initial_step(first_step),
-        rtol=rtol, atol=atol, max_steps=max_steps, mode=mode,
-        n_save_hist=None if options.save_history else 1, grid_blocks=grid_blocks,
-    )
+    n_hist = None if options.save_history else 1
+    common = dict(y0=y0_d, times=t_d, params=p_d, weights=w_d, dt0=initial_step(first_step),
+                  rtol=rtol, atol=atol, max_steps=max_steps, n_save_hist=n_hist)
+    if launch_mode == "auto" and n >= AUTOTUNE_MIN_TRAJECTORIES:
+        from menodax_b200 import autotune
+
+        choice = autotune.tune(ode_fn, n_vars, n_params, options, tune_block=tune_block, **common)
+        options = _replace(options, threads_per_block=choice.threads_per_block)
+        problem = get_problem(ode_fn, n_vars, n_params, options)
+        mode = choice.mode
+        grid_blocks = autotune.grid_blocks(problem, choice, n)
+    else:
+        problem = get_problem(ode_fn, n_vars, n_params, options)
+    hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, **common)
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     if torch_io and input_on_gpu:
         if return_stats:

@@ -26,6 +26,7 @@ from menodax_b200._sparsity import dense_jacobian
 from menodax_b200._trace import trace
 
 TSIT5_EXPONENT = -1.0 / 5.0   # modax/tsit5.py:90
+DENSE_UNROLL_MAX = 12          # mdx_dense_lu.cuh: register-resident dense LU up to this size
 RODAS5P_EXPONENT = -1.0 / 6.0  # modax/rodas5P.py:113
 
 
@@ -52,6 +53,9 @@ class KernelOptions:
     checkpoint: bool = False
     ckpt_stride: int = 1
     adjoint: bool = False
+    # Fast arithmetic for the FP32-LU path: LU in the LU type throughout, the
+    # reciprocal diagonal multiplied in, a float-precision controller exponent.
+    fast: bool = False
 
 
 def controller_exponents(options: KernelOptions):
@@ -113,6 +117,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
         f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
         f"#define MDX_CKPT_SEG {int(options.ckpt_stride)}",
+        f"#define MDX_FAST {1 if options.fast else 0}",
         f"#define MDX_TPB {int(options.threads_per_block)}",
         f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
         '#include "mdx_common.cuh"',
@@ -126,7 +131,22 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     lu_size = 0
     sparse = None
     if rodas:
-        if options.sparsity is None:
+        if options.sparsity is None and options.fast and n_vars <= DENSE_UNROLL_MAX:
+            structure = dense_jacobian(n_vars)
+            lu_size = n_vars * n_vars
+            parts.append(f"#define MDX_LU_SIZE {lu_size}")
+            parts.append(f"#define MDX_IPIV {n_vars}")
+            parts.append('#include "mdx_dense_lu.cuh"')
+            parts.append(
+                "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP& ipiv) "
+                "{ mdx::dense_factorize_fast<MDX_NV, MDX_LU_T>(lu, ipiv); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP& ipiv, R& rhs) "
+                "{ mdx::dense_solve_fast<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP& ipiv, R& rhs) "
+                "{ mdx::dense_solve_t_fast<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "__device__ __forceinline__ int mdx_diag_slot(int d) { return d * MDX_NV + d; }"
+            )
+        elif options.sparsity is None:
             structure = dense_jacobian(n_vars)
             lu_size = n_vars * n_vars
             parts.append(f"#define MDX_LU_SIZE {lu_size}")
@@ -147,7 +167,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
             lu_size = structure.size
             parts.append(f"#define MDX_LU_SIZE {lu_size}")
             parts.append("#define MDX_IPIV 1")
-            parts.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code))
+            parts.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code, fast=options.fast))
             diag = structure.diagonal
             cases = " ".join(f"case {d}: return {int(s)};" for d, s in enumerate(diag))
             parts.append(

@@ -245,7 +245,7 @@ def _c_array(name: str, values) -> str:
     return f"__constant__ int {name}[{max(1, len(values))}] = {{{body}}};"
 
 
-def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto") -> str:
+def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = False) -> str:
     """``mdx_sparse_factorize`` / ``mdx_sparse_solve`` / ``mdx_sparse_solve_t`` for one layout.
 
     ``T`` is the LU element type.  Multipliers and updates run in ``T`` and the
@@ -263,6 +263,9 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto") -> str:
     pivot_of = diag_ptr[layout.col_ind]
     _, updates, substitutions = layout.flop_counts()
     out = []
+    # The reciprocal pivot: double then rounded, as the reference types it; in the
+    # fast path a division in the LU type.
+    recip = "(T)1 / lu[{0}]" if fast else "(T)(1.0 / (double)lu[{0}])"
 
     unroll_factor = mode == "unrolled" or (mode == "auto" and destination.size <= MAX_UNROLLED_UPDATES)
     unroll_solve = mode == "unrolled" or (mode == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS)
@@ -277,7 +280,7 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto") -> str:
                     lines.append(f"  lu[{int(destination[q])}] -= f{p} * lu[{s}];")
                     q += 1
             pivot = int(diag_ptr[i])
-            lines.append(f"  lu[{pivot}] = (T)(1.0 / (double)lu[{pivot}]);")
+            lines.append(f"  lu[{pivot}] = {recip.format(pivot)};")
         out.append(
             "template <typename T, class LU> __device__ __forceinline__ void mdx_sparse_factorize(LU& lu) {\n"
             + "\n".join(lines) + "\n}"
@@ -299,7 +302,7 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto") -> str:
             "      int q = mdx_lu_start[p];\n"
             "      for (int s = above + 1; s < mdx_lu_end[p]; ++s, ++q) lu[mdx_lu_dst[q]] -= f * lu[s];\n"
             "    }\n"
-            "    lu[pivot] = (T)(1.0 / (double)lu[pivot]);\n"
+            f"    lu[pivot] = {recip.format('pivot')};\n"
             "  }\n}"
         )
 

@@ -27,10 +27,19 @@ __device__ __forceinline__ bool finite(double x) { return isfinite(x); }
 
 __device__ __forceinline__ double nan_value() { return __longlong_as_double(0x7ff8000000000000LL); }
 
+// x^e for the step-size factor in the fast path: the factor is a heuristic that
+// is clamped to [0.2, 6] and multiplied by 0.9, so float precision (relative
+// error ~1e-6) is ample; __powf is two special-function-unit instructions.
+__device__ __forceinline__ double fast_pow(double x, double e) {
+  return (double)__powf((float)x, (float)e);
+}
+
 // Step-size controller (modax/rodas5P.py:913-928, modax/tsit5.py:383-398):
 // clamp the error into [1e-18, 1e18] (NaN counts as huge), form the PID factor
 // from the error history, and clamp the factor.  E2 and E3 are compile-time
-// constants, so the default I-controller multiplies by nothing extra.
+// constants, so the default I-controller multiplies by nothing extra.  FAST
+// evaluates the powers in float.
+template <bool FAST>
 __device__ __forceinline__ double controller_factor(double err_norm, double err_prev,
                                                     double err_prev2, double e1, double e2,
                                                     double e3, bool use_e2, bool use_e3,
@@ -41,6 +50,12 @@ __device__ __forceinline__ double controller_factor(double err_norm, double err_
     safe_err = 1e-18;
   } else {
     safe_err = err_norm;
+  }
+  if (FAST) {
+    double factor = 0.9 * fast_pow(safe_err, e1);
+    if (use_e2) factor = factor * fast_pow(err_prev, e2);
+    if (use_e3) factor = factor * fast_pow(err_prev2, e3);
+    return factor;
   }
   double factor = 0.9 * pow(safe_err, e1);
   if (use_e2) factor = factor * pow(err_prev, e2);

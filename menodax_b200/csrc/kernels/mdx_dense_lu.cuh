@@ -164,4 +164,107 @@ __device__ __forceinline__ void dense_solve_t(const LU& lu, const IP& ipiv, R& r
   }
 }
 
+// --- fast arithmetic (MDX_FAST): the FP32-LU path of the persistent kernel ------
+// The factorisation runs entirely in T (no double multipliers, no conversions),
+// the row swaps are folded into a permutation `perm` (perm[i] = the original
+// row that ends at position i) so a solve permutes its right-hand side with
+// selects instead of branches, and the diagonal is left holding 1/U_ii so the
+// back substitution multiplies.  Same algorithm, different rounding: the FP32
+// path is held to accuracy against the FP64 oracle, not to the reference's bits.
+template <int N, typename T, class LU, class IP>
+__device__ __forceinline__ void dense_factorize_fast(LU& lu, IP& perm) {
+  static_assert(N <= MDX_DENSE_UNROLL_MAX, "the fast dense LU is for register-resident systems");
+#pragma unroll
+  for (int i = 0; i < N; ++i) perm[i] = i;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    T max_val = fabs(lu[i * N + i]);
+    int pivot = i;
+#pragma unroll
+    for (int k = i + 1; k < N; ++k) {
+      const T v = fabs(lu[k * N + i]);
+      if (v > max_val) { max_val = v; pivot = k; }
+    }
+#pragma unroll
+    for (int k = i + 1; k < N; ++k) {
+      const bool sw = pivot == k;
+#pragma unroll
+      for (int j = 0; j < N; ++j) {
+        const T a = lu[i * N + j], b = lu[k * N + j];
+        lu[i * N + j] = sw ? b : a;
+        lu[k * N + j] = sw ? a : b;
+      }
+      const int pa = perm[i], pb = perm[k];
+      perm[i] = sw ? pb : pa;
+      perm[k] = sw ? pa : pb;
+    }
+    const T piv = lu[i * N + i];
+    const T inv_piv = piv != T(0) ? T(1) / piv : T(0);
+#pragma unroll
+    for (int k = i + 1; k < N; ++k) {
+      const T factor = lu[k * N + i] * inv_piv;
+      lu[k * N + i] = factor;
+#pragma unroll
+      for (int j = i + 1; j < N; ++j) lu[k * N + j] -= factor * lu[i * N + j];
+    }
+    lu[i * N + i] = T(1) / piv;
+  }
+}
+
+template <int N, typename T, class LU, class IP, class R>
+__device__ __forceinline__ void dense_solve_fast(const LU& lu, const IP& perm, R& rhs) {
+  T x[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    T v = rhs[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) v = perm[i] == k ? rhs[k] : v;
+    x[i] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    T acc = x[i];
+#pragma unroll
+    for (int j = 0; j < i; ++j) acc -= lu[i * N + j] * x[j];
+    x[i] = acc;
+  }
+#pragma unroll
+  for (int i = N - 1; i >= 0; --i) {
+    T acc = x[i];
+#pragma unroll
+    for (int j = i + 1; j < N; ++j) acc -= lu[i * N + j] * x[j];
+    x[i] = acc * lu[i * N + i];
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) rhs[i] = x[i];
+}
+
+// Transposed solve for the fast factorisation: M^T x = b with M = P^T L U.
+template <int N, typename T, class LU, class IP, class R>
+__device__ __forceinline__ void dense_solve_t_fast(const LU& lu, const IP& perm, R& rhs) {
+  T z[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    T acc = rhs[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) acc -= lu[k * N + i] * z[k];
+    z[i] = acc * lu[i * N + i];
+  }
+#pragma unroll
+  for (int i = N - 1; i >= 0; --i) {
+    T acc = z[i];
+#pragma unroll
+    for (int k = i + 1; k < N; ++k) acc -= lu[k * N + i] * z[k];
+    z[i] = acc;
+  }
+  // x[perm[i]] = z[i]
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    T v = z[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i) v = perm[i] == j ? z[i] : v;
+    rhs[j] = perm[0] == j ? z[0] : v;
+  }
+}
+
 }  // namespace mdx

@@ -83,6 +83,14 @@ constexpr double FACTOR_MIN = 0.2;
 constexpr double FACTOR_MAX = 6.0;
 
 typedef MDX_LU_T lu_t;
+// The stage increments are rounded to the LU type when stored (the reference's
+// k_stages, modax/rodas5P.py:724).  Small systems keep the rounded values in
+// double registers, which holds the same numbers without converting on every use.
+#if MDX_NS <= 8
+typedef double k_t;
+#else
+typedef lu_t k_t;
+#endif
 
 struct State {
   double y[MDX_NS];
@@ -170,7 +178,7 @@ __device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& 
   }
   mdx_solve(lu, ipiv, rhs);
 #pragma unroll
-  for (int j = 0; j < MDX_NV; ++j) k[S][j] = rhs[j];
+  for (int j = 0; j < MDX_NV; ++j) k[S][j] = (k_t)rhs[j];
 #if MDX_NSENS > 0
   double kstate[MDX_NV];
 #pragma unroll
@@ -184,7 +192,7 @@ __device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& 
     for (int j = 0; j < MDX_NV; ++j) rhs[j] = (lu_t)(work[base + j] + coupling[s * MDX_NV + j]);
     mdx_solve(lu, ipiv, rhs);
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) k[S][base + j] = rhs[j];
+    for (int j = 0; j < MDX_NV; ++j) k[S][base + j] = (k_t)rhs[j];
   }
 #endif
 }
@@ -207,7 +215,11 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   const double inv_dt = 1.0 / dt_use;
   const double t = st.t;
   const double t_end = t + dt_use;
+#if MDX_FAST
+  const double dtgamma_inv = inv_dt * (1.0 / GAMMA);
+#else
   const double dtgamma_inv = 1.0 / (dt_use * GAMMA);
+#endif
 
   lu_t lu[MDX_LU_SIZE];
   int ipiv[MDX_IPIV];
@@ -218,7 +230,7 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   mdx_factorize(lu, ipiv);
 
   lu_t rhs[MDX_NV];
-  lu_t k[8][MDX_NS];
+  k_t k[8][MDX_NS];
   double u[MDX_NS];
   double work[MDX_NS];
 
@@ -257,12 +269,16 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
     const double r = weight(a, st.traj, j) * (double)k[7][j] / scale;
     err_local += r * r;
   }
+#if MDX_FAST
+  const double err_norm = sqrt(err_local * (1.0 / MDX_NERR));
+#else
   const double err_norm = sqrt(err_local / MDX_NERR);
+#endif
   const bool accept = err_norm <= 1.0 && !isnan(err_norm);
 
   double safe_err;
-  double factor = controller_factor(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2, MDX_E3,
-                                    MDX_USE_E2, MDX_USE_E3, safe_err);
+  double factor = controller_factor<MDX_FAST>(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2,
+                                              MDX_E3, MDX_USE_E2, MDX_USE_E3, safe_err);
   if (accept) {
     st.err_prev2 = st.err_prev;
     st.err_prev = safe_err;

@@ -63,12 +63,18 @@ def solve(
     save_history: bool = True,
     launch: str = "auto",
     sparse_code: str = "auto",
+    arithmetic: str = "auto",
 ):
     """Rodas5P ensemble solve of ``y' = ode_fn(y, t, p)`` on one GPU.
 
     ``lu_precision`` selects the precision of the iteration matrix, its LU and
     the stored stage increments; the state, right-hand side, Jacobian, error and
-    controller are always double.  ``sparsity`` (a mask, a scipy sparse matrix or
+    controller are always double.  ``arithmetic="reference"`` rounds exactly
+    where the reference does (double multipliers in the LU, divisions in the
+    substitutions, a double-precision controller power); ``"fast"`` runs the LU
+    wholly in the LU type with the reciprocal diagonal multiplied in and the
+    controller power in float.  ``"auto"`` is fast for ``lu_precision="fp32"``
+    and reference for ``"fp64"``.  ``sparsity`` (a mask, a scipy sparse matrix or
     ``(nnz, 2)`` pairs) colours the Jacobian sweep and compiles a sparse LU for the
     pattern, ordered by ``ordering`` (``"amd"`` or ``"natural"``).  ``tf_index``
     names a parameter column holding each trajectory's own end time.
@@ -78,6 +84,9 @@ def solve(
     """
     if lu_precision not in LU_PRECISIONS:
         raise ValueError(f"lu_precision must be one of {LU_PRECISIONS}; got {lu_precision!r}")
+    if arithmetic not in ("auto", "reference", "fast"):
+        raise ValueError(f"arithmetic must be 'auto', 'reference' or 'fast'; got {arithmetic!r}")
+    fast = arithmetic == "fast" or (arithmetic == "auto" and lu_precision == "fp32")
     if array_rhs is not None:
         raise NotImplementedError(
             "array_rhs is a numba device function; this build traces ode_fn itself "
@@ -106,6 +115,7 @@ def solve(
         tf_index=-1 if tf_index is None else int(tf_index),
         max_registers=max_registers,
         save_history=bool(save_history),
+        fast=fast,
     )
     from menodax_b200.autograd import needs_grad, solve_with_grad
 
@@ -117,5 +127,5 @@ def solve(
     return run(
         ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
         max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
-        launch_mode=launch,
+        launch_mode=launch, tune_block=trajectories_per_block is None,
     )

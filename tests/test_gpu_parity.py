@@ -59,12 +59,13 @@ def test_tsit5_lorenz_divergence_distribution():
     assert loop.min() == 664 and loop.max() == 735
 
 
-@pytest.mark.parametrize("lu_precision", ["fp64", "fp32"])
-def test_rodas5p_robertson_matches_oracle(oracle, lu_precision):
+@pytest.mark.parametrize("lu_precision,arithmetic", [("fp64", "reference"), ("fp32", "reference"),
+                                                     ("fp32", "fast")])
+def test_rodas5p_robertson_matches_oracle(oracle, lu_precision, arithmetic):
     cfg = systems.robertson_config(size=2048)
     hist, stats = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"],
                                 rtol=cfg["rtol"], atol=cfg["atol"], lu_precision=lu_precision,
-                                return_stats=True, launch="plain")
+                                arithmetic=arithmetic, return_stats=True, launch="plain")
     h, a, r, l = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"],
                               cfg["params"], rtol=cfg["rtol"], atol=cfg["atol"], lu_precision=lu_precision)
     same = _step_match(stats, a, r)
@@ -80,10 +81,11 @@ def test_rodas5p_robertson_matches_oracle(oracle, lu_precision):
         assert abs(gl.mean() - l.mean()) <= 0.02 * l.mean()
 
 
-def test_rodas5p_robertson_fp32_within_10_rtol_of_fp64_oracle(oracle):
+@pytest.mark.parametrize("arithmetic", ["reference", "fast"])
+def test_rodas5p_robertson_fp32_within_10_rtol_of_fp64_oracle(oracle, arithmetic):
     cfg = systems.robertson_config(size=1024)
     hist = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"],
-                         atol=cfg["atol"], lu_precision="fp32")
+                         atol=cfg["atol"], lu_precision="fp32", arithmetic=arithmetic)
     ref, *_ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
                            rtol=1e-12, atol=1e-16, lu_precision="fp64")
     err = np.abs(hist - ref) / (np.abs(ref) + cfg["atol"] / cfg["rtol"])
@@ -96,7 +98,8 @@ def test_rodas5p_robertson_golden_fp32_steps():
     y0 = np.broadcast_to(systems.ROBERTSON_Y0, (n, 3)).copy()
     p = np.broadcast_to(systems.ROBERTSON_PARAMS, (n, 3)).copy()
     _, stats = rodas5P.solve(systems.robertson, y0, systems.ROBERTSON_TIMES, p, rtol=1e-6, atol=1e-8,
-                             first_step=1e-4, lu_precision="fp32", return_stats=True)
+                             first_step=1e-4, lu_precision="fp32", arithmetic="reference",
+                             return_stats=True)
     loop = np.asarray(stats["loop_steps"])
     rej = np.asarray(stats["rejected_steps"])
     assert abs(int(loop[0]) - 157) <= 1 and abs(int(rej[0]) - 10) <= 1

@@ -51,6 +51,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_TRAJ)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the tuned timed launches (for ncu captures); prints no bench line")
+    ap.add_argument("--launch", default="auto", choices=["auto", "plain", "persistent"],
+                    help="launch of the timed kernel (auto = autotuned)")
+    ap.add_argument("--config", default="robertson",
+                    choices=["robertson", "lorenz", "vdp4", "vdp16", "vdp64", "brusselator",
+                             "grad_vdp1", "grad_vdp8"],
+                    help="robertson: the headline line; the others print a line for that configuration")
     return ap.parse_args()
 
 
@@ -266,11 +274,123 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
     }
 
 
+# --------------------------------------------------------------------------- other configurations
+def run_config(args):
+    """One line per non-headline configuration: device-timed solves/s of the
+    autotuned FP32-LU kernel (Tsit5: FP64) and of the plain FP64 reference-
+    arithmetic kernel, plus the step statistics and the CPU oracle on a sample."""
+    import numpy as np
+    import torch
+
+    from menodax_b200 import _native, autotune, systems
+    from menodax_b200._ensemble import launch
+    from menodax_b200._problem import KernelOptions, get_problem
+    from menodax_b200._sparsity import normalize_sparsity
+
+    rank, world, _ = dist_setup(args)
+    if args.config.startswith("grad_"):
+        n_osc = int(args.config[len("grad_vdp"):])
+        n = 65536 if args.n == N_TRAJ else args.n
+        res = measure_gradients(n, args.steps, args.warmup, rank, world, n_osc=n_osc)
+        if rank == 0:
+            print(json.dumps({"config": args.config, **res}))
+        return
+    dev = torch.device("cuda", torch.cuda.current_device())
+    variants = []
+    if args.config == "lorenz":
+        cfg = systems.lorenz_config(size=4096, seed=42 + rank)
+        n_vars, n_params = 3, 1
+        variants = [("tsit5_fp64", KernelOptions(solver="tsit5"))]
+        oracle_sys = ("tsit5", "lorenz", ())
+    elif args.config.startswith("vdp"):
+        n_osc = int(args.config[3:])
+        cfg = systems.vdp_ring_config(n_osc, size=32768, seed=42 + rank)
+        n_vars, n_params = 2 * n_osc, 1
+        pat = normalize_sparsity(cfg["sparsity"], n_vars)
+        variants = [("sparse_fp32_fast", KernelOptions(lu_precision="fp32", fast=True, sparsity=pat))]
+        if n_vars <= 32:
+            variants.append(("dense_fp32", KernelOptions(lu_precision="fp32", fast=n_vars <= 12)))
+            variants.append(("plain_fp64_reference_arith", KernelOptions(lu_precision="fp64")))
+        else:
+            # A dense per-thread LU of 128 states is what the reference's own
+            # benchmark timed out on; the plain baseline here is the sparse FP64 one.
+            variants.append(("plain_fp64_sparse_reference_arith", KernelOptions(lu_precision="fp64", sparsity=pat)))
+        oracle_sys = ("rodas5P", "vdp_ring", (n_osc, 1.0, 0.1))
+    else:
+        cfg = systems.brusselator_config(size=16384, seed=42 + rank)
+        n_vars, n_params = 64, 1
+        pat = normalize_sparsity(cfg["sparsity"], n_vars)
+        variants = [("sparse_fp32_fast", KernelOptions(lu_precision="fp32", fast=True, sparsity=pat)),
+                    ("dense_fp32", KernelOptions(lu_precision="fp32")),
+                    ("plain_fp64_reference_arith", KernelOptions(lu_precision="fp64"))]
+        oracle_sys = ("rodas5P", "brusselator", (32,))
+    if args.n != N_TRAJ:
+        cfg = {**cfg, "y0": cfg["y0"][:args.n], "params": cfg["params"][:args.n]}
+    fn = cfg["ode_fn"]
+    n = cfg["y0"].shape[0]
+    y0 = torch.as_tensor(cfg["y0"], device=dev).contiguous()
+    params = torch.as_tensor(cfg["params"], device=dev).contiguous()
+    times = torch.as_tensor(cfg["t_span"], device=dev).contiguous()
+    common = dict(y0=y0, times=times, params=params, weights=None, dt0=0.0, rtol=cfg["rtol"],
+                  atol=cfg["atol"], max_steps=100000)
+    stream = torch.cuda.current_stream(dev)
+    results = {}
+    stats = None
+    for name, opts in variants:
+        if name.startswith("plain"):
+            prob, mode, grid = get_problem(fn, n_vars, n_params, opts), _native.MDX_LAUNCH_PLAIN, 0
+            label = "plain, 32 threads/block"
+        else:
+            choice = autotune.tune(fn, n_vars, n_params, opts, **common)
+            from dataclasses import replace
+
+            prob = get_problem(fn, n_vars, n_params, replace(opts, threads_per_block=choice.threads_per_block))
+            mode, grid = choice.mode, autotune.grid_blocks(prob, choice, n)
+            label = choice.describe()
+        for _ in range(args.warmup):
+            hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
+        barrier(world)
+        ms = []
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
+            e1.record(stream)
+            ms.append((e0, e1))
+        barrier(world)
+        t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
+        results[name] = {"solves_per_s": n * world * args.steps / (t * 1e-3), "ms_per_solve": t / args.steps,
+                         "launch": label}
+        if stats is None:
+            loop = counters[2].to(torch.float64)
+            stats = {"steps_mean": float(loop.mean()), "steps_max": float(loop.max()),
+                     "max_steps_hit": int((counters[3] & 1).sum())}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+
+        solver, sysname, sysargs = oracle_sys
+        system = getattr(oracle.System, sysname)(*sysargs)
+        sample = 256 if n_vars > 8 else 2048
+        t0 = time.perf_counter()
+        oracle.solve(solver, system, cfg["y0"][:sample], cfg["t_span"], cfg["params"][:sample],
+                     rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp32", threads=oracle.max_threads())
+        cpu = {"value": sample / (time.perf_counter() - t0), "unit": "solves/s",
+               "cores": oracle.max_threads(), "kind": "port", "sample": f"first {sample} trajectories"}
+    if rank == 0:
+        print(json.dumps({"config": args.config, "trajectories": n * world, "n_vars": n_vars,
+                          "variants": results, "step_stats": stats, "cpu_baseline": cpu}))
+
+
 # --------------------------------------------------------------------------- our arm
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.config != "robertson":
+        run_config(args)
         return
     import torch
 
@@ -342,6 +462,10 @@ def main():
     if sampler:
         sampler.start()
         time.sleep(0.3)
+    if args.profile:
+        timed(tuned, choice.mode, args.steps, args.warmup, tuned_grid)
+        print(json.dumps({"profile": "done", "launch": choice.describe()}))
+        return
     ms = timed(tuned, choice.mode, args.steps, args.warmup, tuned_grid)
     clocks = sampler.stop() if sampler else {}
     total_ms = max_over_ranks(sum(ms), world)
@@ -384,14 +508,21 @@ def main():
     t_h = torch.as_tensor(cfg["t_span"]).pin_memory()
     kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp32", return_stats=True,
               launch="auto")
-    for _ in range(args.warmup):
-        rodas5P.solve(fn, y0_h, t_h, p_h, **kw)
+    # Warm-up keeps its results alive the way the timed loop does, so torch's
+    # pinned host allocator holds the two result buffers a steady state needs.
+    out = None
+    for _ in range(max(2, args.warmup)):
+        out, st = rodas5P.solve(fn, y0_h, t_h, p_h, **kw)
     barrier(world)
+    per_call = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        tc = time.perf_counter()
         out, st = rodas5P.solve(fn, y0_h, t_h, p_h, **kw)
+        per_call.append(time.perf_counter() - tc)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    print("e2e per call (ms):", [round(1e3 * x, 3) for x in per_call], file=sys.stderr)
     e2e = n * world * args.steps / e2e_s
     h2d = y0_h.numel() * 8 + p_h.numel() * 8 + t_h.numel() * 8
     d2h = out.numel() * 8 + 3 * n * 4

@@ -10,7 +10,11 @@ launch) on the caller's own inputs -- or on a leading sample of them for large
 ensembles -- and the fastest is remembered per (problem, ensemble size, device).
 
 Candidates: plain and persistent launches at 32, 64 and 128 threads per block,
-the persistent grid at the occupancy limit or half of it.
+the persistent grid at the occupancy limit or half of it.  Tuning is bounded in
+time: a probe solve of the leading ``PROBE`` trajectories estimates the cost of
+a full launch, and when timing every candidate on the whole ensemble would take
+longer than ``BUDGET_S`` the candidates run on a leading sample instead (never
+smaller than ``PROBE``).
 """
 
 from __future__ import annotations
@@ -26,7 +30,8 @@ from menodax_b200._problem import get_problem
 
 BLOCK_SIZES = (32, 64, 128)
 PERSISTENT_FILL = (1.0, 0.5)
-SAMPLE_MAX = 65536
+PROBE = 4096
+BUDGET_S = 3.0
 
 
 @dataclass(frozen=True)
@@ -76,10 +81,26 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
         found = _cache.get(key)
     if found is not None:
         return found
-    m = min(n, SAMPLE_MAX)
+    stream = torch.cuda.current_stream(y0.device)
+    m = n
+    if n > PROBE:
+        prob = get_problem(ode_fn, n_vars, n_params, options)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch(prob, y0=y0[:PROBE], times=times, params=params[:PROBE],
+               weights=weights[:PROBE] if weights is not None else None, dt0=dt0, rtol=rtol,
+               atol=atol, max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN, n_save_hist=n_save_hist)
+        e1.record(stream)
+        e1.synchronize()
+        probe_s = e0.elapsed_time(e1) * 1e-3
+        # A latency-bound launch costs about the same for the probe and a
+        # full-device ensemble, so the probe time bounds one candidate launch.
+        launches = 2 * len(candidates(blocks))
+        if probe_s * launches > BUDGET_S:
+            m = PROBE
     ys, ps = y0[:m], params[:m]
     ws = weights[:m] if weights is not None else None
-    stream = torch.cuda.current_stream(y0.device)
     best = None
     for choice in candidates(blocks):
         prob = get_problem(ode_fn, n_vars, n_params, replace(options, threads_per_block=choice.threads_per_block))

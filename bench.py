@@ -307,14 +307,14 @@ def run_config(args):
         cfg = systems.vdp_ring_config(n_osc, size=32768, seed=42 + rank)
         n_vars, n_params = 2 * n_osc, 1
         pat = normalize_sparsity(cfg["sparsity"], n_vars)
-        variants = [("sparse_fp32_fast", KernelOptions(lu_precision="fp32", fast=True, sparsity=pat))]
+        variants = [("sparse_fp32_fast", KernelOptions(lu_precision="fp32", fast=True, sparsity=pat)),
+                    ("plain_fp64_sparse_reference_arith", KernelOptions(lu_precision="fp64", sparsity=pat))]
         if n_vars <= 32:
+            # Dense per-thread LUs last: at 32 states they dominate the run time,
+            # and at 128 (what the reference's own benchmark timed out on) they
+            # are not run.
             variants.append(("dense_fp32", KernelOptions(lu_precision="fp32", fast=n_vars <= 12)))
             variants.append(("plain_fp64_reference_arith", KernelOptions(lu_precision="fp64")))
-        else:
-            # A dense per-thread LU of 128 states is what the reference's own
-            # benchmark timed out on; the plain baseline here is the sparse FP64 one.
-            variants.append(("plain_fp64_sparse_reference_arith", KernelOptions(lu_precision="fp64", sparsity=pat)))
         oracle_sys = ("rodas5P", "vdp_ring", (n_osc, 1.0, 0.1))
     else:
         cfg = systems.brusselator_config(size=16384, seed=42 + rank)
@@ -362,6 +362,8 @@ def run_config(args):
         t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
         results[name] = {"solves_per_s": n * world * args.steps / (t * 1e-3), "ms_per_solve": t / args.steps,
                          "launch": label}
+        if rank == 0:
+            print(json.dumps({"config": args.config, "variant": name, **results[name]}), flush=True)
         if stats is None:
             loop = counters[2].to(torch.float64)
             stats = {"steps_mean": float(loop.mean()), "steps_max": float(loop.max()),

@@ -76,8 +76,14 @@ def initial_step(first_step) -> float:
     return 0.0 if first_step is None else float(first_step)
 
 
-def solver_stats(accepted, rejected, loop_steps):
-    return {"accepted_steps": accepted, "rejected_steps": rejected, "loop_steps": loop_steps}
+def solver_stats(accepted, rejected, loop_steps, status=None):
+    """The reference's stats dict (``modax/_numba_common.py:133-138``), plus the
+    per-trajectory status bits when available (1: max_steps reached before the last
+    save, 2: non-finite final state, 4: checkpoint capacity exceeded)."""
+    stats = {"accepted_steps": accepted, "rejected_steps": rejected, "loop_steps": loop_steps}
+    if status is not None:
+        stats["status"] = status
+    return stats
 
 
 def pick_device(*tensors):

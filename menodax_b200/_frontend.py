@@ -89,14 +89,14 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     if torch_io and input_on_gpu:
         if return_stats:
-            return hist, solver_stats(counters[0], counters[1], counters[2])
+            return hist, solver_stats(counters[0], counters[1], counters[2], counters[3])
         return hist
-    hist_h, counters_h = _to_host(hist, counters[:3] if return_stats else None)
+    hist_h, counters_h = _to_host(hist, counters if return_stats else None)
     if not torch_io:
         hist_h = hist_h.numpy()
         counters_h = counters_h.numpy() if counters_h is not None else None
     if return_stats:
-        return hist_h, solver_stats(counters_h[0], counters_h[1], counters_h[2])
+        return hist_h, solver_stats(counters_h[0], counters_h[1], counters_h[2], counters_h[3])
     return hist_h
 
 

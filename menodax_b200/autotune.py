@@ -14,7 +14,9 @@ the persistent grid at the occupancy limit or half of it.  Tuning is bounded in
 time: a probe solve of the leading ``PROBE`` trajectories estimates the cost of
 a full launch, and when timing every candidate on the whole ensemble would take
 longer than ``BUDGET_S`` the candidates run on a leading sample instead (never
-smaller than ``PROBE``).
+smaller than ``PROBE``).  When even that would blow the budget tenfold, no
+candidate is timed: uneven step counts in the probe (max over mean above 2)
+choose the persistent refill launch at half fill, even ones the plain launch.
 """
 
 from __future__ import annotations
@@ -88,15 +90,25 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        launch(prob, y0=y0[:PROBE], times=times, params=params[:PROBE],
-               weights=weights[:PROBE] if weights is not None else None, dt0=dt0, rtol=rtol,
-               atol=atol, max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN, n_save_hist=n_save_hist)
+        _, counters = launch(prob, y0=y0[:PROBE], times=times, params=params[:PROBE],
+                             weights=weights[:PROBE] if weights is not None else None, dt0=dt0,
+                             rtol=rtol, atol=atol, max_steps=max_steps,
+                             mode=_native.MDX_LAUNCH_PLAIN, n_save_hist=n_save_hist)
         e1.record(stream)
         e1.synchronize()
         probe_s = e0.elapsed_time(e1) * 1e-3
         # A latency-bound launch costs about the same for the probe and a
         # full-device ensemble, so the probe time bounds one candidate launch.
         launches = 2 * len(candidates(blocks))
+        if probe_s * launches > 10 * BUDGET_S:
+            steps = counters[2].to(torch.float64)
+            uneven = float(steps.max()) > 2.0 * float(steps.mean())
+            tpb = options.threads_per_block if not tune_block else 64
+            choice = (LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5) if uneven
+                      else LaunchChoice(options.threads_per_block, _native.MDX_LAUNCH_PLAIN, 0.0))
+            with _lock:
+                _cache[key] = choice
+            return choice
         if probe_s * launches > BUDGET_S:
             m = PROBE
     ys, ps = y0[:m], params[:m]

@@ -1,0 +1,46 @@
+"""API validation that needs no GPU: the reference's error messages and argument
+normalisation (modax/_jax_common.py:23-36, modax/rodas5P.py:1204-1211)."""
+
+import numpy as np
+import pytest
+
+from menodax_b200 import _ensemble, rodas5P, systems, tsit5
+
+
+def test_shape_errors():
+    with pytest.raises(ValueError, match="y0 must have shape"):
+        rodas5P.solve(systems.robertson, np.zeros((2, 3, 1)), systems.ROBERTSON_TIMES, np.zeros(3))
+    with pytest.raises(ValueError, match="params must have shape"):
+        rodas5P.solve(systems.robertson, np.zeros((2, 3)), systems.ROBERTSON_TIMES, np.zeros((3, 3)))
+
+
+def test_option_errors():
+    with pytest.raises(ValueError, match="lu_precision"):
+        rodas5P.solve(systems.robertson, np.zeros(3), systems.ROBERTSON_TIMES, np.zeros(3), lu_precision="fp16")
+    with pytest.raises(ValueError, match="save_history=False"):
+        rodas5P.solve(systems.robertson, np.zeros(3), systems.ROBERTSON_TIMES, np.zeros(3), save_history=False)
+    with pytest.raises(ValueError, match="positive hook_size"):
+        rodas5P.solve(systems.robertson, np.zeros(3), systems.ROBERTSON_TIMES, np.zeros(3),
+                      save_hook=lambda *a: None)
+    with pytest.raises(ValueError, match="trajectories_per_block must be positive"):
+        rodas5P.trajectories_per_block_or_default(0)
+    with pytest.raises(ValueError, match="backend must be"):
+        tsit5.solve(systems.lorenz, np.zeros(3), (0.0, 1.0), np.zeros(1), backend="gpu")
+    with pytest.raises(ValueError, match="shared backend requires"):
+        tsit5.solve(systems.make_vdp_system(16)[0], np.zeros(32), (0.0, 1.0), np.zeros(1), backend="shared")
+
+
+def test_normalisation_broadcasts():
+    y0, p, n, nv = _ensemble.normalize_y0_params(np.ones(3), np.ones((5, 2)))
+    assert (n, nv) == (5, 3) and tuple(y0.shape) == (5, 3) and tuple(p.shape) == (5, 2)
+    y0, p, n, nv = _ensemble.normalize_y0_params(np.ones((4, 2)), np.ones(1))
+    assert n == 4 and tuple(p.shape) == (4, 1)
+    assert _ensemble.initial_step(None) == 0.0 and _ensemble.initial_step(1e-3) == 1e-3
+    assert _ensemble.build_error_weights(None, 4, 2) is None
+    w = _ensemble.build_error_weights([1.0, 0.0], 4, 2)
+    assert tuple(w.shape) == (4, 2)
+
+
+def test_trajectories_per_block_default():
+    assert rodas5P.trajectories_per_block_or_default() == 32
+    assert rodas5P.trajectories_per_block_or_default(8) == 8

@@ -150,3 +150,32 @@ def test_common_subexpressions_collapse():
     tr = trace(fn, 2, 0)
     muls = [nd for nd in tr.graph.nodes if nd.op == "mul"]
     assert len(muls) == 2  # y0*y1 once, then a*b
+
+
+def test_sensitivity_spec_sizes():
+    """tests/test_sensitivity.py:124-161 in the reference: only requested blocks count."""
+    from menodax_b200.sensitivity import SensitivitySpec
+
+    params_only = SensitivitySpec(n_vars=4, n_params=2, wrt_y0=False, wrt_params=True)
+    assert params_only.n_sens == 2 and params_only.n_aug == 12 and params_only.n_error == 12
+    both = SensitivitySpec(n_vars=4, n_params=2, wrt_y0=True, wrt_params=True, error_control=False)
+    assert both.n_sens == 6 and both.n_aug == 28 and both.n_error == 4
+    cols = SensitivitySpec(n_vars=3, n_params=5, wrt_y0=False, wrt_params=True, param_columns=(4, 1))
+    assert cols.param_seed_columns == (4, 1) and cols.n_sens == 2
+    with pytest.raises(ValueError, match="at least one"):
+        SensitivitySpec(n_vars=2, n_params=1, wrt_y0=False, wrt_params=False)
+    with pytest.raises(ValueError, match="repeat"):
+        SensitivitySpec(n_vars=2, n_params=3, wrt_y0=False, wrt_params=True, param_columns=(1, 1))
+
+
+def test_augmented_layout():
+    import torch
+
+    from menodax_b200.sensitivity import SensitivitySpec, augmented_y0, split_augmented
+
+    spec = SensitivitySpec(n_vars=2, n_params=1, wrt_y0=True, wrt_params=True)
+    z = augmented_y0(torch.tensor([[1.0, 2.0]]), spec)
+    assert z.tolist() == [[1.0, 2.0, 1.0, 0.0, 0.0, 1.0, 0.0, 0.0]]
+    state, sens = split_augmented(z.reshape(1, 1, -1), spec)
+    assert state.tolist() == [[[1.0, 2.0]]]
+    assert sens[0, 0].tolist() == [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]

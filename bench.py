@@ -132,43 +132,21 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- helpers
 def dist_setup(args):
-    import torch
+    from menodax_b200 import _dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
-    return rank, world, local
+    return _dist.init(backend="nccl")
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from menodax_b200 import _dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _dist.max_over_ranks(x, world)
 
 
 def barrier(world):
-    import torch
+    from menodax_b200 import _dist
 
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-    torch.cuda.synchronize()
+    _dist.barrier(world)
 
 
 def cpu_sample_solve(cfg, n_sample, lu_precision):
@@ -561,10 +539,9 @@ def main():
             "gpu_launches": args.steps,
         }
         print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
+    from menodax_b200 import _dist
 
-        dist.destroy_process_group()
+    _dist.finalize(world)
 
 
 if __name__ == "__main__":

@@ -44,6 +44,8 @@ extern "C" {
 
 #define MDX_PLAN_CHECKPOINT 1   /* the module records accepted step states */
 #define MDX_PLAN_ADJOINT 2      /* the module carries the discrete-adjoint kernel */
+#define MDX_PLAN_SAVE_HOOK 4    /* the module calls a save hook: hook_out is required */
+#define MDX_PLAN_NO_HISTORY 8   /* the module keeps only the final state: n_save_hist == 1 */
 
 /* Per-trajectory status bits written to mdx_solve_desc.status. */
 #define MDX_STATUS_OK 0
@@ -91,7 +93,7 @@ typedef struct mdx_solve_desc {
   int* rejected;          /* (n_traj,) */
   int* loop_steps;        /* (n_traj,) */
   int* status;            /* (n_traj,) or NULL */
-  double* hook_out;       /* reserved, NULL */
+  double* hook_out;       /* MDX_PLAN_SAVE_HOOK: (n_traj, hook_size), zeroed and filled by the kernel */
   const int* order;       /* persistent: optional trajectory visiting order, or NULL */
   void* workspace;        /* persistent: >= mdx_workspace_size() bytes */
   size_t workspace_bytes;

@@ -78,7 +78,21 @@ class Emitter:
             name = self.names.get(kind)
             if name is None:
                 raise KeyError(f"no C name bound for variable kind {kind!r}")
-            self.done[nid] = name if kind == "t" else f"{name}[{idx}]"
+            if callable(name):
+                self.done[nid] = name(idx)
+            else:
+                self.done[nid] = name if kind in ("t", "sidx") else f"{name}[{idx}]"
+            return
+        if op == "table":
+            tid, off = node.payload
+            nm = f"{self.prefix}{nid}"
+            self.lines.append(f"  const double {nm} = mdx_hook_table{tid}[save_idx + ({off})];")
+            self.done[nid] = nm
+            return
+        if op == "accdyn":
+            nm = f"{self.prefix}{nid}"
+            self.lines.append(f"  const double {nm} = acc[save_idx + ({node.payload})];")
+            self.done[nid] = nm
             return
         a = [self.done[x] for x in node.args]
         if op == "add":
@@ -282,3 +296,28 @@ def emit_adjoint_pieces(tr: TracedRHS) -> str:
         + f"#define MDX_AUTONOMOUS {0 if any(x is not None for x in ft) else 1}\n"
     )
     return "\n".join(out)
+
+
+def emit_save_hook(th) -> str:
+    """``mdx_save_hook(save_idx, y, t, p, acc)``: every read of ``acc`` sees the row
+    as it was on entry (loaded first), the stores follow in program order."""
+    g = th.graph
+    parts = []
+    for tid, vals in enumerate(th.tables):
+        body = ",".join(lit(float(v)) for v in vals) or "0.0"
+        parts.append(f"__constant__ double mdx_hook_table{tid}[{max(1, len(vals))}] = {{{body}}};")
+    em = Emitter(g, {"y": "y", "t": "t", "p": "p", "sidx": "(double)save_idx",
+                     "acc": lambda k: f"acc_in{k}"}, prefix="h")
+    slots = sorted({nd.payload[1] for nd in g.nodes if nd.op == "var" and nd.payload[0] == "acc"})
+    loads = [f"  const double acc_in{k} = acc[{k}];" for k in slots]
+    values = [em.expr(node) for _, node in th.stores]
+    stores = []
+    for (slot, _), val in zip(th.stores, values):
+        target = f"acc[save_idx + ({slot[1]})]" if isinstance(slot, tuple) else f"acc[{slot}]"
+        stores.append(f"  {target} = {val};")
+    parts.append(
+        "template <class Y>\n"
+        "__device__ __forceinline__ void mdx_save_hook(const int save_idx, const Y& y, const double t, "
+        "const double* p, double* acc) {\n" + "\n".join(loads + em.lines + stores) + "\n}\n"
+    )
+    return "\n".join(parts)

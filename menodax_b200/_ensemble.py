@@ -123,7 +123,7 @@ class Workspace:
 
 def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, mode,
            n_save_hist=None, grid_blocks=0, order=None, ckpt=None, ckpt_count=None,
-           ckpt_capacity=0, out=None):
+           ckpt_capacity=0, out=None, hook_out=None):
     """Allocate outputs on ``y0``'s device and launch one ensemble solve.
 
     All inputs must already be contiguous float64 CUDA tensors on one device.
@@ -158,6 +158,7 @@ def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, m
     desc.loop_steps = counters[2].data_ptr()
     desc.status = counters[3].data_ptr()
     desc.order = order.data_ptr() if order is not None else None
+    desc.hook_out = hook_out.data_ptr() if hook_out is not None else None
     stream = torch.cuda.current_stream(dev).cuda_stream
     if mode == _native.MDX_LAUNCH_PERSISTENT:
         nbytes = problem.plan.workspace_size(mode, n)

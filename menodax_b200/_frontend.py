@@ -75,7 +75,10 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     n_hist = None if options.save_history else 1
     common = dict(y0=y0_d, times=t_d, params=p_d, weights=w_d, dt0=initial_step(first_step),
                   rtol=rtol, atol=atol, max_steps=max_steps, n_save_hist=n_hist)
-    if launch_mode == "auto" and n >= AUTOTUNE_MIN_TRAJECTORIES:
+    hook_out = None
+    if options.save_hook is not None:
+        hook_out = torch.empty((n, options.hook_size), dtype=torch.float64, device=device)
+    if launch_mode == "auto" and n >= AUTOTUNE_MIN_TRAJECTORIES and hook_out is None:
         from menodax_b200 import autotune
 
         choice = autotune.tune(ode_fn, n_vars, n_params, options, tune_block=tune_block, **common)
@@ -85,19 +88,33 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
         grid_blocks = autotune.grid_blocks(problem, choice, n)
     else:
         problem = get_problem(ode_fn, n_vars, n_params, options)
-    hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, **common)
+    n_save = int(t_d.shape[0])
+    for name, length, lo, hi in problem.hook_tables:
+        if lo < 0 or n_save - 1 + hi >= length:
+            raise ValueError(
+                f"the save hook reads or writes {name} at save_idx + {hi if lo >= 0 else lo}, "
+                f"outside its {length} entries for {n_save} save times"
+            )
+    hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, hook_out=hook_out, **common)
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     if torch_io and input_on_gpu:
+        result = (hist,) if hook_out is None else (hist, hook_out)
         if return_stats:
-            return hist, solver_stats(counters[0], counters[1], counters[2], counters[3])
-        return hist
+            result += (solver_stats(counters[0], counters[1], counters[2], counters[3]),)
+        return result[0] if len(result) == 1 else result
     hist_h, counters_h = _to_host(hist, counters if return_stats else None)
+    hook_h = None
+    if hook_out is not None:
+        hook_h = torch.empty(hook_out.shape, dtype=hook_out.dtype, pin_memory=True)
+        hook_h.copy_(hook_out)
     if not torch_io:
         hist_h = hist_h.numpy()
         counters_h = counters_h.numpy() if counters_h is not None else None
+        hook_h = hook_h.numpy() if hook_h is not None else None
+    result = (hist_h,) if hook_h is None else (hist_h, hook_h)
     if return_stats:
-        return hist_h, solver_stats(counters_h[0], counters_h[1], counters_h[2], counters_h[3])
-    return hist_h
+        result += (solver_stats(counters_h[0], counters_h[1], counters_h[2], counters_h[3]),)
+    return result[0] if len(result) == 1 else result
 
 
 def _to_host(hist, counters):

@@ -31,6 +31,8 @@ MDX_LAUNCH_PLAIN = 0
 MDX_LAUNCH_PERSISTENT = 1
 MDX_PLAN_CHECKPOINT = 1
 MDX_PLAN_ADJOINT = 2
+MDX_PLAN_SAVE_HOOK = 4
+MDX_PLAN_NO_HISTORY = 8
 MDX_STATUS_MAX_STEPS = 1
 MDX_STATUS_NONFINITE = 2
 MDX_STATUS_CKPT_OVERFLOW = 4

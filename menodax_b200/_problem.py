@@ -17,13 +17,14 @@ from menodax_b200._codegen import (
     emit_adjoint_pieces,
     emit_neg_jac,
     emit_rhs,
+    emit_save_hook,
     emit_sens_coupling,
     lit,
 )
 from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
 from menodax_b200._sparse_direct import sparse_direct_solver_for
 from menodax_b200._sparsity import dense_jacobian
-from menodax_b200._trace import trace
+from menodax_b200._trace import trace, trace_hook
 
 TSIT5_EXPONENT = -1.0 / 5.0   # modax/tsit5.py:90
 DENSE_UNROLL_MAX = 12          # mdx_dense_lu.cuh: register-resident dense LU up to this size
@@ -56,6 +57,10 @@ class KernelOptions:
     # Fast arithmetic for the FP32-LU path: LU in the LU type throughout, the
     # reciprocal diagonal multiplied in, a float-precision controller exponent.
     fast: bool = False
+    # A save hook hook(save_idx, y, t, p_row, acc) traced into the kernel, and the
+    # width of its per-trajectory output row (modax/rodas5P.py:157-164).
+    save_hook: object = None
+    hook_size: int = 0
 
 
 def controller_exponents(options: KernelOptions):
@@ -79,6 +84,7 @@ class Problem:
     options: KernelOptions
     lu_size: int
     sparse: object = None
+    hook_tables: tuple = ()
 
 
 def _sens_layout(n_vars, n_params, sens):
@@ -118,6 +124,8 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
         f"#define MDX_CKPT_SEG {int(options.ckpt_stride)}",
         f"#define MDX_FAST {1 if options.fast else 0}",
+        f"#define MDX_HAS_HOOK {1 if options.save_hook is not None else 0}",
+        f"#define MDX_HOOK_SIZE {max(1, int(options.hook_size))}",
         f"#define MDX_TPB {int(options.threads_per_block)}",
         f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
         '#include "mdx_common.cuh"',
@@ -180,11 +188,18 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 f"__device__ __forceinline__ int mdx_diag_slot(int d) {{ switch (d) {{ {cases} default: return 0; }} }}"
             )
         parts.append(emit_neg_jac(tr, structure, lu_size, sens))
+        if options.save_hook is not None:
+            hook = trace_hook(options.save_hook, n_system, n_params, int(options.hook_size))
+            parts.append(emit_save_hook(hook))
+            meta_tables = hook.bounds()
+        else:
+            meta_tables = []
         if sens is not None:
             parts.append(emit_sens_coupling(tr, sens))
         parts.append('#include "mdx_rodas5p.cuh"')
         parts.append("#define MDX_SOLVER mdx::Rodas5P")
     else:
+        meta_tables = []
         parts.append("#define MDX_LU_SIZE 1")
         parts.append('#include "mdx_tsit5.cuh"')
         parts.append("#define MDX_SOLVER mdx::Tsit5")
@@ -195,7 +210,8 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         parts.append(emit_adjoint_pieces(tr))
         parts.append("#define MDX_ADJOINT_RODAS5P" if rodas else "#define MDX_ADJOINT_TSIT5")
         parts.append('#include "mdx_adjoint.cuh"')
-    meta = dict(n_system=n_system, n_error=n_error, lu_size=lu_size, sparse=sparse)
+    meta = dict(n_system=n_system, n_error=n_error, lu_size=lu_size, sparse=sparse,
+                hook_tables=meta_tables)
     return "\n".join(parts) + "\n", meta
 
 
@@ -221,6 +237,8 @@ def get_problem(ode_fn, n_vars: int, n_params: int, options: KernelOptions) -> P
     cubin = _native.compile_cubin(source, compile_options(options))
     flags = (_native.MDX_PLAN_CHECKPOINT if options.checkpoint else 0) | (
         _native.MDX_PLAN_ADJOINT if options.adjoint else 0
+    ) | (_native.MDX_PLAN_SAVE_HOOK if options.save_hook is not None else 0) | (
+        0 if options.save_history else _native.MDX_PLAN_NO_HISTORY
     )
     solver = _native.MDX_SOLVER_TSIT5 if options.solver == "tsit5" else _native.MDX_SOLVER_RODAS5P
     plan = _native.Plan(solver, n_vars, meta["n_system"], n_params, options.threads_per_block, flags, cubin,
@@ -228,6 +246,7 @@ def get_problem(ode_fn, n_vars: int, n_params: int, options: KernelOptions) -> P
     prob = Problem(
         plan=plan, source=source, n_vars=n_vars, n_system=meta["n_system"], n_params=n_params,
         n_error=meta["n_error"], options=options, lu_size=meta["lu_size"], sparse=meta["sparse"],
+        hook_tables=tuple(meta["hook_tables"]),
     )
     with _cache_lock:
         _cache.setdefault(key, prob)

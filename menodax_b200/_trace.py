@@ -237,6 +237,8 @@ class Graph:
             node = self.nodes[nid]
             if node.op == "const":
                 tangent[nid] = None
+            elif node.op in ("table", "accdyn"):
+                tangent[nid] = None
             elif node.op == "var":
                 tangent[nid] = seeds.get(nid)
             else:
@@ -577,3 +579,147 @@ def evaluate(traced: TracedRHS, y, t, p):
                 folded = float("nan")
             vals[nid] = folded
     return [vals[o] for o in traced.outputs]
+
+
+# --- save hooks -----------------------------------------------------------------------
+class SaveIndex:
+    """The save index a hook receives: usable as an index (``acc[save_idx]``,
+    ``table[save_idx + 1]``) and, lifted to a float, in arithmetic."""
+
+    def __init__(self, g: Graph, offset: int = 0):
+        self.g = g
+        self.offset = int(offset)
+
+    def __add__(self, other):
+        if isinstance(other, int) and not isinstance(other, bool):
+            return SaveIndex(self.g, self.offset + other)
+        return self._as_sym() + other
+
+    __radd__ = __add__
+
+    def __sub__(self, other):
+        if isinstance(other, int) and not isinstance(other, bool):
+            return SaveIndex(self.g, self.offset - other)
+        return self._as_sym() - other
+
+    def _as_sym(self):
+        s = Sym(self.g, self.g.var("sidx"))
+        return s + float(self.offset) if self.offset else s
+
+    def __mul__(self, other):
+        return self._as_sym() * other
+
+    __rmul__ = __mul__
+
+    def __float__(self):
+        raise TraceError("use the save index as an index, or in arithmetic with traced values")
+
+    def __index__(self):
+        raise TraceError("the save index is only known on the device; index acc or a table with it")
+
+
+class _Table:
+    """A host array a hook closes over, readable at literal or save-index positions."""
+
+    def __init__(self, g: Graph, tables: list, values):
+        import numpy as np
+
+        self.g = g
+        self.values = np.asarray(values, dtype=np.float64).ravel()
+        self.tid = len(tables)
+        tables.append(self.values)
+
+    def __getitem__(self, index):
+        if isinstance(index, SaveIndex):
+            return Sym(self.g, self.g._add(Node("table", (), (self.tid, index.offset))))
+        return Sym(self.g, self.g.const(float(self.values[operator.index(index)])))
+
+    def __len__(self):
+        return len(self.values)
+
+
+class _Accumulator:
+    """The hook's output row: reads see the row as it was when the hook was
+    called, writes are applied in program order when it returns."""
+
+    def __init__(self, g: Graph, size: int):
+        self.g = g
+        self.size = size
+        self.current: dict[int, object] = {}
+        self.stores: list = []  # (slot or ("dyn", offset), node)
+
+    def _slot(self, index):
+        if isinstance(index, SaveIndex):
+            return ("dyn", index.offset)
+        i = operator.index(index)
+        if not 0 <= i < self.size:
+            raise TraceError(f"acc[{i}] is outside the hook's {self.size} slots")
+        return i
+
+    def __getitem__(self, index):
+        slot = self._slot(index)
+        if slot in self.current:
+            return self.current[slot]
+        if isinstance(slot, tuple):
+            return Sym(self.g, self.g._add(Node("accdyn", (), slot[1])))
+        return Sym(self.g, self.g.var("acc", slot))
+
+    def __setitem__(self, index, value):
+        slot = self._slot(index)
+        node = value.nid if isinstance(value, Sym) else self.g.const(float(value))
+        self.current[slot] = Sym(self.g, node)
+        self.stores.append((slot, node))
+
+    def __len__(self):
+        return self.size
+
+
+@dataclass
+class TracedHook:
+    graph: Graph
+    stores: list
+    tables: list
+    hook_size: int
+
+    def bounds(self):
+        """``(name, length, min offset, max offset)`` of every save-index access."""
+        out = []
+        for node in self.graph.nodes:
+            if node.op == "table":
+                tid, off = node.payload
+                out.append((f"table {tid}", len(self.tables[tid]), off, off))
+            elif node.op == "accdyn":
+                out.append(("acc", self.hook_size, node.payload, node.payload))
+        for slot, _ in self.stores:
+            if isinstance(slot, tuple):
+                out.append(("acc", self.hook_size, slot[1], slot[1]))
+        return out
+
+
+def trace_hook(hook, n_system: int, n_params: int, hook_size: int) -> TracedHook:
+    """Run a save hook ``hook(save_idx, y, t, p_row, acc)`` on proxies."""
+    import numpy as np
+
+    g = Graph()
+    tables: list = []
+    fn = _with_shimmed_globals(hook)
+    if isinstance(fn, types.FunctionType):
+        # Arrays the hook closes over or reads as globals become device tables.
+        def wrap(v):
+            if isinstance(v, np.ndarray) or type(v).__name__ == "Tensor":
+                return _Table(g, tables, v.detach().cpu().numpy() if hasattr(v, "detach") else v)
+            return v
+
+        glb = {k: wrap(v) for k, v in fn.__globals__.items()}
+        cells = None
+        if fn.__closure__:
+            cells = tuple(types.CellType(wrap(c.cell_contents)) for c in fn.__closure__)
+        fn = types.FunctionType(fn.__code__, glb, fn.__name__, fn.__defaults__, cells)
+    acc = _Accumulator(g, hook_size)
+    try:
+        fn(SaveIndex(g), _Vector(g, "y", n_system), Sym(g, g.var("t")), _Vector(g, "p", n_params), acc)
+    except TraceError:
+        raise
+    except TypeError as exc:
+        raise TraceError(f"tracing the save hook failed: {exc}") from exc
+    return TracedHook(graph=g, stores=acc.stores, tables=tables, hook_size=hook_size)

@@ -144,6 +144,14 @@ __device__ __forceinline__ void init(State& st, const MdxSolveArgs& a, int traj)
   st.n_ckpt = 0;
   st.ckpt_overflow = false;
 #endif
+#if MDX_HAS_HOOK
+  // The hook's row starts at zero and accumulates over the trajectory's saves
+  // (modax/rodas5P.py:753-756).
+  double* acc = a.hook_out + (size_t)traj * MDX_HOOK_SIZE;
+#pragma unroll 1
+  for (int j = 0; j < MDX_HOOK_SIZE; ++j) acc[j] = 0.0;
+  mdx_save_hook(0, st.y, t0, st.p, acc);
+#endif
 }
 
 __device__ __forceinline__ bool running(const State& st, const MdxSolveArgs& a) {
@@ -300,6 +308,9 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
     while (st.save_idx < a.n_save && save_reached(a.times[st.save_idx], t_new)) {
       const double theta = (a.times[st.save_idx] - t) / dt_use;
       const double theta1 = 1.0 - theta;
+#if MDX_HAS_HOOK
+      double y_save[MDX_NS];
+#endif
 #pragma unroll
       for (int j = 0; j < MDX_NS; ++j) {
         double h1 = coef_h(0, 0) * (double)k[0][j];
@@ -316,7 +327,14 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
 #if MDX_SAVE_HISTORY
         a.hist[hist_index(a, st.traj, st.save_idx, j)] = val;
 #endif
+#if MDX_HAS_HOOK
+        y_save[j] = val;
+#endif
       }
+#if MDX_HAS_HOOK
+      mdx_save_hook(st.save_idx, y_save, a.times[st.save_idx], st.p,
+                    a.hook_out + (size_t)st.traj * MDX_HOOK_SIZE);
+#endif
       ++st.save_idx;
     }
 #pragma unroll
@@ -337,6 +355,10 @@ __device__ __forceinline__ void finish(State& st, const MdxSolveArgs& a) {
 #if MDX_SAVE_HISTORY
 #pragma unroll
     for (int j = 0; j < MDX_NS; ++j) a.hist[hist_index(a, st.traj, st.save_idx, j)] = st.y[j];
+#endif
+#if MDX_HAS_HOOK
+    mdx_save_hook(st.save_idx, st.y, a.times[st.save_idx], st.p,
+                  a.hook_out + (size_t)st.traj * MDX_HOOK_SIZE);
 #endif
     ++st.save_idx;
   }

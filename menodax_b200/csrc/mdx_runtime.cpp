@@ -319,14 +319,17 @@ int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, in
     return fail(MDX_E_INVALID, "mdx_solve_desc.struct_size %d != %d", d->struct_size, (int)sizeof(mdx_solve_desc));
   if (d->n_traj < 0) return fail(MDX_E_INVALID, "n_traj must be non-negative; got %d", d->n_traj);
   if (d->n_save < 1) return fail(MDX_E_INVALID, "times must hold at least one value; got %d", d->n_save);
-  if (d->n_save_hist != d->n_save && d->n_save_hist != 1)
-    return fail(MDX_E_INVALID, "n_save_hist must be n_save or 1; got %d", d->n_save_hist);
   if (d->mode != MDX_LAUNCH_PLAIN && d->mode != MDX_LAUNCH_PERSISTENT)
     return fail(MDX_E_INVALID, "unknown launch mode %d", d->mode);
   if (d->n_traj == 0) return MDX_OK;
   if (!d->y0 || !d->times || (plan->desc.n_params > 0 && !d->params) || !d->hist || !d->accepted ||
       !d->rejected || !d->loop_steps)
     return fail(MDX_E_INVALID, "mdx_solve: a required buffer is NULL");
+  if ((plan->desc.flags & MDX_PLAN_SAVE_HOOK) && !d->hook_out)
+    return fail(MDX_E_INVALID, "the plan calls a save hook: hook_out must not be NULL");
+  if ((plan->desc.flags & MDX_PLAN_NO_HISTORY) ? d->n_save_hist != 1 : d->n_save_hist != d->n_save)
+    return fail(MDX_E_INVALID, "n_save_hist %d does not match the plan's history (%s)", d->n_save_hist,
+                (plan->desc.flags & MDX_PLAN_NO_HISTORY) ? "final state only" : "every save");
   const bool ckpt = (plan->desc.flags & MDX_PLAN_CHECKPOINT) != 0;
   if (ckpt && (!d->ckpt || !d->ckpt_count || d->ckpt_capacity < 1))
     return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt, ckpt_count and ckpt_capacity >= 1");

@@ -79,6 +79,16 @@ def solve(
     pattern, ordered by ``ordering`` (``"amd"`` or ``"natural"``).  ``tf_index``
     names a parameter column holding each trajectory's own end time.
 
+    ``save_hook(save_idx, y, t, p_row, acc)`` runs inside the kernel at every save
+    (the initial state, each dense-output save, the frozen saves past a
+    trajectory's end) on the state at that time; it is traced like ``ode_fn``:
+    ``acc`` is the trajectory's ``hook_size``-wide row, zeroed at the start,
+    indexed with literals or with ``save_idx`` (plus a literal offset), and host
+    arrays it closes over may be indexed with ``save_idx`` too.  A hooked solve
+    returns ``(hist, hook_out)`` (plus the stats when asked); with
+    ``save_history=False`` ``hist`` keeps only the final state, shape
+    ``(N, 1, n_vars)`` (``modax/rodas5P.py:1161-1171``).
+
     Torch inputs that require grad are differentiated by the discrete adjoint
     (checkpointed step states, reverse sweep on the device).
     """
@@ -95,8 +105,7 @@ def solve(
     if save_hook is not None:
         if hook_size <= 0:
             raise ValueError("a save_hook needs a positive hook_size")
-        raise NotImplementedError("save_hook is not supported by this build")
-    if not save_history:
+    elif not save_history:
         raise ValueError("save_history=False needs a save_hook to consume the saves")
     n_vars = int(torch.as_tensor(y0).shape[-1]) if not hasattr(y0, "shape") else int(y0.shape[-1])
     if sparsity is not None:
@@ -116,10 +125,14 @@ def solve(
         max_registers=max_registers,
         save_history=bool(save_history),
         fast=fast,
+        save_hook=save_hook,
+        hook_size=int(hook_size) if save_hook is not None else 0,
     )
     from menodax_b200.autograd import needs_grad, solve_with_grad
 
     if needs_grad(y0, params):
+        if save_hook is not None:
+            raise NotImplementedError("a solve with a save_hook is not differentiable")
         return solve_with_grad(
             ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
             max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,

@@ -124,3 +124,51 @@ def test_torch_device_inputs_stay_on_device():
     assert isinstance(out, torch.Tensor) and out.is_cuda
     ref = tsit5.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"], atol=cfg["atol"])
     assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_error_weights_match_oracle(oracle):
+    """A zero weight drops a component from step-size control (modax/rodas5P.py:1072-1074)."""
+    cfg = systems.robertson_config(size=256)
+    w = np.array([1.0, 0.0, 1.0])
+    hist, stats = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"],
+                                atol=cfg["atol"], lu_precision="fp64", error_weights=w,
+                                return_stats=True, launch="plain")
+    h, a, r, _ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
+                              rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64", error_weights=w)
+    same = _step_match(stats, a, r)
+    assert same.mean() >= 0.999
+    _states_agree(hist, h, same, atol=1e-15)
+
+
+def test_tf_index_ends_each_trajectory_at_its_own_time():
+    """tests/test_solver_options.py:66-93 in the reference."""
+    t_span = np.linspace(0.0, 1.0, 11)
+    params = np.array([[10.0, 5.0, 1.0], [10.0, 5.0, 0.5]])
+    out = rodas5P.solve(systems.forced_decay, np.zeros((2, 1)), t_span, params, tf_index=2, rtol=1e-10,
+                        atol=1e-12, first_step=1e-4, lu_precision="fp64")
+    exact = 5.0 * (10.0 * t_span - 1.0 + np.exp(-10.0 * t_span)) / 100.0
+    np.testing.assert_allclose(out[0, :, 0], exact, rtol=1e-8, atol=1e-10)
+    stops = int(np.searchsorted(t_span, 0.5, side="right"))
+    np.testing.assert_allclose(out[1, :stops, 0], exact[:stops], rtol=1e-8, atol=1e-10)
+    assert (out[1, stops:, 0] == out[1, stops - 1, 0]).all()
+
+
+def test_the_time_derivative_term_reaches_the_stages():
+    """tests/test_solver_options.py:40-63 in the reference."""
+    t_span = np.linspace(0.0, 1.0, 11)
+    out = rodas5P.solve(systems.forced_decay, np.zeros((1, 1)), t_span, np.array([[10.0, 5.0]]),
+                        rtol=1e-10, atol=1e-12, first_step=1e-4, lu_precision="fp64")
+    exact = 5.0 * (10.0 * t_span - 1.0 + np.exp(-10.0 * t_span)) / 100.0
+    np.testing.assert_allclose(out[0, :, 0], exact, rtol=1e-8, atol=1e-10)
+
+
+@pytest.mark.parametrize("solve", [tsit5.solve, rodas5P.solve])
+def test_default_first_step_matches_explicit(solve):
+    """tests/test_solvers.py:71-96: first_step=None is 1e-6 of the window."""
+    fn, _ = systems.make_vdp_system(1, mu=1.0)
+    y0, p = systems.vdp_divergence_scenario(1, 8, divergence=1.0)
+    t = systems.VDP_TIMES
+    kw = dict(rtol=1e-6, atol=1e-8)
+    explicit = solve(fn, y0, t, p, first_step=(t[-1] - t[0]) * 1e-6, **kw)
+    default = solve(fn, y0, t, p, **kw)
+    assert np.array_equal(default, explicit)

@@ -242,6 +242,33 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
     total = max_over_ranks(sum(per), world)
     acc = stats["accepted_steps"].to(torch.float64)
     finite = bool(torch.isfinite(gy).all() and torch.isfinite(gp).all())
+
+    # The reference's method on the same GPU: forward sensitivities (the joint
+    # [y, S] solve with the sensitivities under error control, its default),
+    # contracted with the loss's cotangent.
+    from menodax_b200 import sensitivity
+
+    def forward_sensitivity_grad():
+        state, sens = sensitivity.solve("rodas5P", fn, y0, t, mu, **kw)
+        resid = state - target
+        g = torch.einsum("nsj,nsjk->nk", 2.0 * resid, sens)
+        return (resid ** 2).sum(), g
+
+    fs_steps = max(1, steps // 2)
+    forward_sensitivity_grad()
+    barrier(world)
+    fms = []
+    for _ in range(fs_steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, g_fs = forward_sensitivity_grad()
+        e1.record(stream)
+        fms.append((e0, e1))
+    barrier(world)
+    fs_total = max_over_ranks(sum(a.elapsed_time(b) for a, b in fms), world)
+    g_adj = torch.cat([gy, gp], dim=1)
+    rel = ((g_adj - g_fs).abs().max(dim=1).values / g_fs.abs().max(dim=1).values.clamp_min(1e-300))
     return {
         "metric": "gradients/s", "value": n * world * steps / (total * 1e-3), "unit": "gradients/s",
         "ms_per_step": total / steps,
@@ -249,6 +276,11 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
                     f"{n} trajectories per GPU, 20 saves on [0, 1000], rtol 1e-6, atol 1e-8",
         "accepted_steps_mean": float(acc.mean()), "accepted_steps_max": float(acc.max()),
         "gradients_finite": finite,
+        "forward_sensitivities": {
+            "value": n * world * fs_steps / (fs_total * 1e-3), "unit": "gradients/s",
+            "method": "joint [y, S] Rodas5P solve, sensitivities under error control (the reference's method)",
+            "median_rel_diff_vs_adjoint": float(rel.median()),
+        },
     }
 
 

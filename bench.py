@@ -351,10 +351,11 @@ def run_config(args):
             prob, mode, grid = get_problem(fn, n_vars, n_params, opts), _native.MDX_LAUNCH_PLAIN, 0
             label = "plain, 32 threads/block"
         else:
-            choice = autotune.tune(fn, n_vars, n_params, opts, **common)
+            choice = autotune.tune(fn, n_vars, n_params, opts, tune_team=True, **common)
             from dataclasses import replace
 
-            prob = get_problem(fn, n_vars, n_params, replace(opts, threads_per_block=choice.threads_per_block))
+            prob = get_problem(fn, n_vars, n_params,
+                               replace(opts, threads_per_block=choice.threads_per_block, team=choice.team))
             mode, grid = choice.mode, autotune.grid_blocks(prob, choice, n)
             label = choice.describe()
         for _ in range(args.warmup):

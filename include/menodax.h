@@ -39,8 +39,11 @@ extern "C" {
 #define MDX_SOLVER_TSIT5 1
 #define MDX_SOLVER_RODAS5P 2
 
-#define MDX_LAUNCH_PLAIN 0      /* one trajectory per thread, grid = ceil(N / tpb) */
+#define MDX_LAUNCH_PLAIN 0      /* one trajectory per thread (or team) for its whole life */
 #define MDX_LAUNCH_PERSISTENT 1 /* device-sized grid, warps refill from a queue */
+
+/* Largest dynamic shared memory per block a plan may ask for (sm_100 opt-in). */
+#define MDX_MAX_SHARED_BYTES (227 * 1024)
 
 #define MDX_PLAN_CHECKPOINT 1   /* the module records accepted step states */
 #define MDX_PLAN_ADJOINT 2      /* the module carries the discrete-adjoint kernel */
@@ -68,6 +71,10 @@ typedef struct mdx_plan_desc {
   int threads_per_block;  /* the block size the module was compiled for */
   int flags;              /* MDX_PLAN_* */
   int ckpt_stride;        /* MDX_PLAN_CHECKPOINT: steps per recorded start state (>= 1) */
+  int team_size;          /* lanes per trajectory: 1 for the thread-per-trajectory kernels, 4, 8,
+                             16 or 32 for a team module (threads_per_block / team_size
+                             trajectories per block) */
+  int shared_bytes;       /* dynamic shared memory per block the module's solve kernels take */
   const void* cubin;
   size_t cubin_size;
 } mdx_plan_desc;

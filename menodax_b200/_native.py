@@ -33,6 +33,7 @@ MDX_PLAN_CHECKPOINT = 1
 MDX_PLAN_ADJOINT = 2
 MDX_PLAN_SAVE_HOOK = 4
 MDX_PLAN_NO_HISTORY = 8
+MDX_MAX_SHARED_BYTES = 227 * 1024
 MDX_STATUS_MAX_STEPS = 1
 MDX_STATUS_NONFINITE = 2
 MDX_STATUS_CKPT_OVERFLOW = 4
@@ -53,6 +54,7 @@ class PlanDesc(ctypes.Structure):
         ("struct_size", ctypes.c_int), ("solver", ctypes.c_int), ("n_vars", ctypes.c_int),
         ("n_system", ctypes.c_int), ("n_params", ctypes.c_int),
         ("threads_per_block", ctypes.c_int), ("flags", ctypes.c_int), ("ckpt_stride", ctypes.c_int),
+        ("team_size", ctypes.c_int), ("shared_bytes", ctypes.c_int),
         ("cubin", ctypes.c_void_p), ("cubin_size", ctypes.c_size_t),
     ]
 
@@ -211,11 +213,13 @@ class Plan:
     """Owns one ``mdx_plan``: a compiled problem, loaded lazily per CUDA context."""
 
     def __init__(self, solver: int, n_vars: int, n_system: int, n_params: int, tpb: int,
-                 flags: int, cubin: bytes, ckpt_stride: int = 1):
+                 flags: int, cubin: bytes, ckpt_stride: int = 1, team_size: int = 1,
+                 shared_bytes: int = 0):
         self._cubin = ctypes.create_string_buffer(cubin, len(cubin))
         desc = PlanDesc(
             struct_size=ctypes.sizeof(PlanDesc), solver=solver, n_vars=n_vars, n_system=n_system,
             n_params=n_params, threads_per_block=tpb, flags=flags, ckpt_stride=ckpt_stride,
+            team_size=team_size, shared_bytes=shared_bytes,
             cubin=ctypes.cast(self._cubin, ctypes.c_void_p), cubin_size=len(cubin),
         )
         handle = ctypes.c_void_p()
@@ -223,6 +227,8 @@ class Plan:
         self.handle = handle
         self.tpb = tpb
         self.flags = flags
+        self.team_size = team_size
+        self.shared_bytes = shared_bytes
         self._lib = lib()
 
     def __del__(self):

@@ -21,8 +21,10 @@ from menodax_b200._codegen import (
     emit_sens_coupling,
     lit,
 )
+from menodax_b200._sparse_direct import MAX_UNROLLED_SUBSTITUTIONS, sparse_direct_solver_for
 from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._team import TEAM_SIZES, dense_lda, emit_team_functions
+from menodax_b200._team import slice_bytes as team_slice_bytes
 from menodax_b200._sparsity import dense_jacobian
 from menodax_b200._trace import trace, trace_hook
 
@@ -61,6 +63,9 @@ class KernelOptions:
     # width of its per-trajectory output row (modax/rodas5P.py:157-164).
     save_hook: object = None
     hook_size: int = 0
+    # Lanes per trajectory: 0 for the thread-per-trajectory kernels, else 4, 8,
+    # 16 or 32 for the team kernel (Rodas5P, no sensitivities, hooks or adjoint).
+    team: int = 0
 
 
 def controller_exponents(options: KernelOptions):
@@ -94,9 +99,127 @@ def _sens_layout(n_vars, n_params, sens):
     return SensLayout(n_vars, n_params, n_y0_dirs, tuple(cols))
 
 
+def team_block_threads(n_vars: int, n_params: int, options: KernelOptions, preferred: int = 128) -> int:
+    """Threads per block for a team launch: ``preferred`` or fewer, whole warps, and
+    no more trajectories than a block's shared memory holds (a bound that assumes
+    the slice carries ``df/dt``)."""
+    team = int(options.team)
+    lu_bytes = 4 if options.lu_precision == "fp32" else 8
+    dense = options.sparsity is None
+    if dense:
+        lu_size = n_vars * dense_lda(n_vars)
+    else:
+        lu_size = sparse_direct_solver_for(options.sparsity, options.ordering).compressed.size
+    per = team_slice_bytes(n_vars, n_params, lu_size, lu_bytes, dense=dense, autonomous=False,
+                           fast=options.fast)
+    fit = max(1, _native.MDX_MAX_SHARED_BYTES // per)
+    threads = min(preferred // team, fit) * team
+    threads = threads // 32 * 32
+    if threads < 32:
+        if 32 // team > fit:
+            raise ValueError(f"a warp of {team}-lane teams needs {32 // team} slices of {per} B; "
+                             "they exceed a block's shared memory")
+        threads = 32
+    return threads
+
+
+def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
+    """The team kernel's source: class loops for f, -J and df/dt, the matrix in shared memory."""
+    if options.solver != "rodas5P":
+        raise ValueError("the team kernel runs Rodas5P")
+    if options.team not in TEAM_SIZES:
+        raise ValueError(f"team must be one of {TEAM_SIZES}; got {options.team}")
+    if options.sens is not None or options.save_hook is not None or options.checkpoint or options.adjoint:
+        raise ValueError("the team kernel integrates the plain system: no sens, save_hook, checkpoint or adjoint")
+    tpb = int(options.threads_per_block)
+    if tpb % 32 or tpb % options.team:
+        raise ValueError(f"threads_per_block {tpb} is not a whole number of warps")
+    lu_t = "float" if options.lu_precision == "fp32" else "double"
+    lu_bytes = 4 if lu_t == "float" else 8
+    e1, e2, e3 = controller_exponents(options)
+    dense = options.sparsity is None
+    extra = []
+    if dense:
+        structure = dense_jacobian(n_vars)
+        lda = dense_lda(n_vars)
+        lu_size = n_vars * lda
+        code = emit_team_functions(tr, structure, lambda row, col: row * lda + col, skip_zero=True)
+        clear = "-0.0"
+        extra.append(f"#define MDX_TEAM_LDA {lda}")
+        extra.append("__device__ __forceinline__ int mdx_team_diag_slot(int d) { return d * MDX_TEAM_LDA + d; }")
+        sparse = None
+        sparse_registers = 0
+    else:
+        sparse = sparse_direct_solver_for(options.sparsity, options.ordering)
+        structure = sparse.compressed
+        lu_size = structure.size
+        store = structure.store_slots()
+
+        def lu_slot(row, colour):
+            slot = int(store[row * structure.n_colours + colour])
+            return None if slot < 0 else slot
+
+        code = emit_team_functions(tr, structure, lu_slot, skip_zero=False)
+        clear = "0.0"
+        diag = ", ".join(str(int(d)) for d in structure.diagonal)
+        extra.append(f"__device__ const int mdx_team_diag[{n_vars}] = {{{diag}}};")
+        extra.append("__device__ __forceinline__ int mdx_team_diag_slot(int d) { return mdx_team_diag[d]; }")
+        extra.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code, fast=options.fast))
+        substitutions = sparse.layout.flop_counts()[2]
+        sparse_registers = int(options.sparse_code == "unrolled" or (
+            options.sparse_code == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS))
+    slice_size = team_slice_bytes(n_vars, n_params, lu_size, lu_bytes, dense=dense,
+                                  autonomous=code.autonomous, fast=options.fast)
+    shared = slice_size * (tpb // options.team)
+    if shared > _native.MDX_MAX_SHARED_BYTES:
+        raise ValueError(
+            f"{tpb // options.team} trajectories of {slice_size} B exceed a block's shared memory; "
+            "use fewer threads per block or a larger team")
+    parts = [
+        f"// generated problem source: rodas5P team kernel, n_vars={n_vars}, n_params={n_params}, "
+        f"team={options.team}, {'dense' if dense else 'sparse'}",
+        f"#define MDX_NV {n_vars}",
+        f"#define MDX_NS {n_vars}",
+        f"#define MDX_NP {n_params}",
+        "#define MDX_NSENS 0",
+        f"#define MDX_NERR {lit(float(n_vars))}",
+        f"#define MDX_LU_T {lu_t}",
+        f"#define MDX_TF_INDEX {int(options.tf_index)}",
+        f"#define MDX_E1 {lit(e1)}",
+        f"#define MDX_E2 {lit(e2)}",
+        f"#define MDX_E3 {lit(e3)}",
+        f"#define MDX_USE_E2 {'true' if e2 != 0.0 else 'false'}",
+        f"#define MDX_USE_E3 {'true' if e3 != 0.0 else 'false'}",
+        f"#define MDX_WEIGHTS_RUNTIME {1 if options.runtime_weights else 0}",
+        f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
+        "#define MDX_CHECKPOINT 0",
+        "#define MDX_HAS_HOOK 0",
+        f"#define MDX_FAST {1 if options.fast else 0}",
+        f"#define MDX_TPB {tpb}",
+        f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
+        f"#define MDX_TEAM {int(options.team)}",
+        f"#define MDX_TEAM_DENSE {1 if dense else 0}",
+        f"#define MDX_TEAM_LU_SIZE {lu_size}",
+        f"#define MDX_TEAM_LU_CLEAR {clear}",
+        f"#define MDX_TEAM_SLICE_BYTES {slice_size}",
+        f"#define MDX_TEAM_SPARSE_REGISTERS {sparse_registers}",
+        '#include "mdx_common.cuh"',
+        "__device__ __forceinline__ double mdx_const_weight(int) { return 1.0; }",
+        code.source,
+        *extra,
+        '#include "mdx_team.cuh"',
+    ]
+    meta = dict(n_system=n_vars, n_error=n_vars, lu_size=lu_size, sparse=sparse, hook_tables=[],
+                shared_bytes=shared, slice_bytes=slice_size, rhs_classes=code.n_rhs_classes,
+                jac_classes=code.n_jac_classes)
+    return "\n".join(parts) + "\n", meta
+
+
 def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     """Generate the full NVRTC source; returns ``(source, meta)``."""
     tr = trace(ode_fn, n_vars, n_params)
+    if options.team:
+        return _build_team_source(tr, n_vars, n_params, options)
     sens = _sens_layout(n_vars, n_params, options.sens)
     n_sens = 0 if sens is None else sens.n_sens
     n_system = n_vars * (1 + n_sens)
@@ -211,7 +334,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         parts.append("#define MDX_ADJOINT_RODAS5P" if rodas else "#define MDX_ADJOINT_TSIT5")
         parts.append('#include "mdx_adjoint.cuh"')
     meta = dict(n_system=n_system, n_error=n_error, lu_size=lu_size, sparse=sparse,
-                hook_tables=meta_tables)
+                hook_tables=meta_tables, shared_bytes=0)
     return "\n".join(parts) + "\n", meta
 
 
@@ -242,7 +365,8 @@ def get_problem(ode_fn, n_vars: int, n_params: int, options: KernelOptions) -> P
     )
     solver = _native.MDX_SOLVER_TSIT5 if options.solver == "tsit5" else _native.MDX_SOLVER_RODAS5P
     plan = _native.Plan(solver, n_vars, meta["n_system"], n_params, options.threads_per_block, flags, cubin,
-                        ckpt_stride=int(options.ckpt_stride))
+                        ckpt_stride=int(options.ckpt_stride), team_size=max(1, int(options.team)),
+                        shared_bytes=int(meta["shared_bytes"]))
     prob = Problem(
         plan=plan, source=source, n_vars=n_vars, n_system=meta["n_system"], n_params=n_params,
         n_error=meta["n_error"], options=options, lu_size=meta["lu_size"], sparse=meta["sparse"],

@@ -10,13 +10,22 @@ launch) on the caller's own inputs -- or on a leading sample of them for large
 ensembles -- and the fastest is remembered per (problem, ensemble size, device).
 
 Candidates: plain and persistent launches at 32, 64 and 128 threads per block,
-the persistent grid at the occupancy limit or half of it.  Tuning is bounded in
-time: a probe solve of the leading ``PROBE`` trajectories estimates the cost of
-a full launch, and when timing every candidate on the whole ensemble would take
-longer than ``BUDGET_S`` the candidates run on a leading sample instead (never
-smaller than ``PROBE``).  When even that would blow the budget tenfold, no
-candidate is timed: uneven step counts in the probe (max over mean above 2)
-choose the persistent refill launch at half fill, even ones the plain launch.
+the persistent grid at the occupancy limit or half of it; for systems of
+``TEAM_MIN_VARS`` states or more, also the team kernel (a team of 8 to 32 lanes
+per trajectory, its vectors and matrix in shared memory), plain and persistent.
+The thread kernel is a candidate up to ``THREAD_MAX_VARS`` states with a sparse
+LU, and for dense LUs only while the matrix stays in registers
+(``DENSE_UNROLL_MAX``): past that its matrix lives in local memory and a team is
+faster by an order of magnitude.
+
+Tuning is bounded in time.  The first candidate runs on the leading ``PROBE``
+trajectories with at most ``PROBE_STEPS`` steps each.  When that finishes every
+trajectory, its time bounds a launch, and the candidates are timed on the whole
+ensemble, or on the probe set when that would exceed ``BUDGET_S``.  When it hits
+the step cap the integrations are long (tens of thousands of steps): the plain
+candidates are ranked by the capped probe, which measures the cost of a step
+with the device full, and the winner runs as a persistent refill launch, since
+long stiff ensembles have uneven step counts.
 """
 
 from __future__ import annotations
@@ -28,12 +37,16 @@ import torch
 
 from menodax_b200 import _native
 from menodax_b200._ensemble import launch
-from menodax_b200._problem import get_problem
+from menodax_b200._problem import DENSE_UNROLL_MAX, get_problem, team_block_threads
+from menodax_b200._team import TEAM_SIZES
 
 BLOCK_SIZES = (32, 64, 128)
 PERSISTENT_FILL = (1.0, 0.5)
 PROBE = 4096
+PROBE_STEPS = 500
 BUDGET_S = 3.0
+TEAM_MIN_VARS = 16
+THREAD_MAX_VARS = 128
 
 
 @dataclass(frozen=True)
@@ -41,23 +54,36 @@ class LaunchChoice:
     threads_per_block: int
     mode: int
     grid_fill: float  # persistent: fraction of the occupancy-limited grid
+    team: int = 0     # lanes per trajectory; 0 = one thread per trajectory
 
     def describe(self) -> str:
         kind = "plain" if self.mode == _native.MDX_LAUNCH_PLAIN else f"persistent(fill={self.grid_fill})"
-        return f"{kind}, {self.threads_per_block} threads/block"
+        lanes = f", team of {self.team}" if self.team else ""
+        return f"{kind}, {self.threads_per_block} threads/block{lanes}"
+
+
 
 
 _cache: dict = {}
 _lock = threading.Lock()
 
 
-def candidates(block_sizes=BLOCK_SIZES):
+def candidates(block_sizes=BLOCK_SIZES, teams=()):
+    """Thread-kernel launches per block size; team launches as ``(team, threads_per_block)`` pairs."""
     out = []
     for tpb in block_sizes:
         out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0))
         for fill in PERSISTENT_FILL:
             out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill))
+    for team, tpb in teams:
+        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, team))
+        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, 1.0, team))
     return out
+
+
+def team_sizes_for(n_vars: int):
+    """Teams worth timing: no wider than the system's state (rounded up to a power of two)."""
+    return tuple(t for t in TEAM_SIZES if t // 2 < n_vars)
 
 
 def grid_blocks(problem, choice: LaunchChoice, n: int) -> int:
@@ -65,72 +91,117 @@ def grid_blocks(problem, choice: LaunchChoice, n: int) -> int:
         return 0
     per_sm, sms = problem.plan.occupancy(choice.mode)
     full = max(1, per_sm) * sms
-    needed = (n + choice.threads_per_block - 1) // choice.threads_per_block
+    per_block = choice.threads_per_block // max(1, choice.team)
+    needed = (n + per_block - 1) // per_block
     return max(1, int(min(full, needed) * choice.grid_fill))
 
 
+def _timed_launch(problem, choice, stream, *, n, y0, times, params, weights, dt0, rtol, atol, max_steps,
+                  n_save_hist):
+    kw = dict(y0=y0[:n], times=times, params=params[:n], weights=weights[:n] if weights is not None else None,
+              dt0=dt0, rtol=rtol, atol=atol, max_steps=max_steps, mode=choice.mode, n_save_hist=n_save_hist,
+              grid_blocks=grid_blocks(problem, choice, n))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, counters = launch(problem, **kw)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, counters
+
+
 def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, rtol, atol,
-         max_steps, n_save_hist=None, tune_block=True):
+         max_steps, n_save_hist=None, tune_block=True, tune_team=False):
     """The fastest launch for this problem on these inputs (device tensors).
 
     With ``tune_block=False`` the block size stays ``options.threads_per_block``
-    and only the launch kind and grid are chosen."""
+    and only the launch kind and grid are chosen.  With ``tune_team`` the team
+    kernel is a candidate too (for systems of ``TEAM_MIN_VARS`` states or more);
+    an ``options.team`` already set is kept and only its launch kind is tuned.
+
+    The first candidate runs once on the leading ``PROBE`` trajectories with at
+    most ``PROBE_STEPS`` steps each.  If that finished every trajectory, its time
+    bounds a launch and the candidates are timed on the whole ensemble (or on
+    the probe set, to stay within ``BUDGET_S``).  If it hit the step cap, the
+    integrations are long: the plain launches are ranked by the same capped
+    probe -- the cost per step with the device full -- and the winner runs as a
+    persistent launch, which refills lanes as the uneven trajectories finish."""
     n = y0.shape[0]
-    blocks = BLOCK_SIZES if tune_block else (options.threads_per_block,)
-    key = (ode_fn, n_vars, n_params, replace(options, threads_per_block=32), n, blocks,
-           torch.cuda.get_device_name(y0.device))
+    if options.team:
+        blocks, teams = (), ((options.team, options.threads_per_block),)
+    else:
+        sizes = team_sizes_for(n_vars) if tune_team and n_vars >= TEAM_MIN_VARS else ()
+        teams = []
+        for t in sizes:
+            try:
+                teams.append((t, team_block_threads(n_vars, n_params, replace(options, team=t))))
+            except ValueError:
+                continue
+        thread_ok = n_vars <= THREAD_MAX_VARS and (options.sparsity is not None or n_vars <= DENSE_UNROLL_MAX)
+        if teams and not thread_ok:
+            blocks = ()
+        else:
+            blocks = BLOCK_SIZES if tune_block else (options.threads_per_block,)
+    cands = candidates(blocks, teams)
+    key = (ode_fn, n_vars, n_params, replace(options, threads_per_block=32, team=0), n, tuple(cands),
+           max_steps, torch.cuda.get_device_name(y0.device))
     with _lock:
         found = _cache.get(key)
     if found is not None:
         return found
+
+    def problem_for(choice):
+        return get_problem(ode_fn, n_vars, n_params,
+                           replace(options, threads_per_block=choice.threads_per_block, team=choice.team))
+
+    buildable = []
+    for choice in cands:
+        try:
+            problem_for(choice)
+        except ValueError:  # a team slice too large for a block's shared memory
+            continue
+        buildable.append(choice)
+    if not buildable:
+        raise ValueError("no launch candidate fits this problem")
     stream = torch.cuda.current_stream(y0.device)
-    m = n
-    if n > PROBE:
-        prob = get_problem(ode_fn, n_vars, n_params, options)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        _, counters = launch(prob, y0=y0[:PROBE], times=times, params=params[:PROBE],
-                             weights=weights[:PROBE] if weights is not None else None, dt0=dt0,
-                             rtol=rtol, atol=atol, max_steps=max_steps,
-                             mode=_native.MDX_LAUNCH_PLAIN, n_save_hist=n_save_hist)
-        e1.record(stream)
-        e1.synchronize()
-        probe_s = e0.elapsed_time(e1) * 1e-3
-        # A latency-bound launch costs about the same for the probe and a
-        # full-device ensemble, so the probe time bounds one candidate launch.
-        launches = 2 * len(candidates(blocks))
-        if probe_s * launches > 10 * BUDGET_S:
-            steps = counters[2].to(torch.float64)
-            uneven = float(steps.max()) > 2.0 * float(steps.mean())
-            tpb = options.threads_per_block if not tune_block else 64
-            choice = (LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5) if uneven
-                      else LaunchChoice(options.threads_per_block, _native.MDX_LAUNCH_PLAIN, 0.0))
-            with _lock:
-                _cache[key] = choice
-            return choice
-        if probe_s * launches > BUDGET_S:
-            m = PROBE
-    ys, ps = y0[:m], params[:m]
-    ws = weights[:m] if weights is not None else None
+    inputs = dict(y0=y0, times=times, params=params, weights=weights, dt0=dt0, rtol=rtol, atol=atol,
+                  n_save_hist=n_save_hist)
+    m = min(n, PROBE)
+    cap = min(int(max_steps), PROBE_STEPS)
+    first = buildable[0]
+    probe_s, counters = _timed_launch(problem_for(replace(first, mode=_native.MDX_LAUNCH_PLAIN, grid_fill=0.0)),
+                                      replace(first, mode=_native.MDX_LAUNCH_PLAIN, grid_fill=0.0), stream,
+                                      n=m, max_steps=cap, **inputs)
+    capped = cap < int(max_steps) and int(counters[2].max()) >= cap
+    if capped:
+        best = None
+        for choice in buildable:
+            if choice.mode != _native.MDX_LAUNCH_PLAIN:
+                continue
+            prob = problem_for(choice)
+            _timed_launch(prob, choice, stream, n=m, max_steps=cap, **inputs)
+            secs, _ = _timed_launch(prob, choice, stream, n=m, max_steps=cap, **inputs)
+            if best is None or secs < best[0]:
+                best = (secs, choice)
+        winner = best[1]
+        fill = 1.0 if winner.team else 0.5
+        persistent = [c for c in buildable if c.mode == _native.MDX_LAUNCH_PERSISTENT and c.team == winner.team
+                      and c.threads_per_block == winner.threads_per_block and c.grid_fill == fill]
+        choice = persistent[0] if persistent else winner
+        with _lock:
+            _cache[key] = choice
+        return choice
+    # The probe ran to completion; a latency-bound launch costs about the same
+    # for the probe set and a full-device ensemble, so it bounds one candidate.
+    launches = 2 * len(buildable)
+    sample = n if probe_s * launches <= BUDGET_S else m
     best = None
-    for choice in candidates(blocks):
-        prob = get_problem(ode_fn, n_vars, n_params, replace(options, threads_per_block=choice.threads_per_block))
-        kw = dict(y0=ys, times=times, params=ps, weights=ws, dt0=dt0, rtol=rtol, atol=atol,
-                  max_steps=max_steps, mode=choice.mode, n_save_hist=n_save_hist,
-                  grid_blocks=grid_blocks(prob, choice, m))
-        launch(prob, **kw)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        launch(prob, **kw)
-        e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        if best is None or ms < best[0]:
-            best = (ms, choice)
+    for choice in buildable:
+        prob = problem_for(choice)
+        _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, **inputs)
+        secs, _ = _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, **inputs)
+        if best is None or secs < best[0]:
+            best = (secs, choice)
     with _lock:
         _cache[key] = best[1]
     return best[1]
-
-

@@ -20,67 +20,10 @@
 // forward sensitivities, mdx_sens_coupling).
 #pragma once
 #include "mdx_common.cuh"
+#include "mdx_rodas5p_coef.cuh"
 
 namespace mdx {
 namespace rodas5p {
-
-// W-transformed Rodas5P coefficients (Steinebach 2023, BIT 63:27), as tabulated
-// in modax/rodas5P.py:44-105.  Stages 6-8 accumulate into u (FSAL form), so only
-// five rows of A exist.
-constexpr double GAMMA = 0.21193756319429014;
-__host__ __device__ constexpr double coef_a(int s, int m) {
-  constexpr double t[5][5] = {
-    {3.0, 0, 0, 0, 0},
-    {2.849394379747939, 0.45842242204463923, 0, 0, 0},
-    {-6.954028509809101, 2.489845061869568, -10.358996098473584, 0, 0},
-    {2.8029986275628964, 0.5072464736228206, -0.3988312541770524, -0.04721187230404641, 0},
-    {-7.502846399306121, 2.561846144803919, -11.627539656261098, -0.18268767659942256,
-     0.030198172008377946},
-};
-  return t[s][m];
-}
-__host__ __device__ constexpr double coef_c(int s, int m) {
-  constexpr double t[8][7] = {
-    {0, 0, 0, 0, 0, 0, 0},
-    {-14.155112264123755, 0, 0, 0, 0, 0, 0},
-    {-17.97296035885952, -2.859693295451294, 0, 0, 0, 0, 0},
-    {147.12150275711716, -1.41221402718213, 71.68940251302358, 0, 0, 0, 0},
-    {165.43517024871676, -0.4592823456491126, 42.90938336958603, -5.961986721573306, 0, 0, 0},
-    {24.854864614690072, -3.0009227002832186, 47.4931110020768, 5.5814197821558125,
-     -0.6610691825249471, 0, 0},
-    {30.91273214028599, -3.1208243349937974, 77.79954646070892, 34.28646028294783,
-     -19.097331116725623, -28.087943162872662, 0},
-    {37.80277123390563, -3.2571969029072276, 112.26918849496327, 66.9347231244047,
-     -40.06618937091002, -54.66780262877968, -9.48861652309627},
-};
-  return t[s][m];
-}
-// Stage abscissae of stages 2..5; stage 1 sits at t, stages 6..8 at t + h.
-__host__ __device__ constexpr double coef_ct(int s) {
-  constexpr double t[4] = {0.6358126895828704, 0.4095798393397535, 0.9769306725060716,
-                          0.4288403609558664};
-  return t[s];
-}
-// df/dt coefficients d_i (zero for stages 6..8).
-__host__ __device__ constexpr double coef_d(int s) {
-  constexpr double t[8] = {GAMMA, -0.42387512638858027, -0.3384627126235924, 1.8046452872882734,
-                         2.325825639765069, 0.0, 0.0, 0.0};
-  return t[s];
-}
-// Continuous extension: h1..h3 as combinations of k1..k8 (modax/rodas5P.py:939-968).
-__host__ __device__ constexpr double coef_h(int r, int m) {
-  constexpr double t[3][8] = {
-    {25.948786856663858, -2.5579724845846235, 10.433815404888879, -2.3679251022685204,
-     0.524948541321073, 1.1241088310450404, 0.4272876194431874, -0.17202221070155493},
-    {-9.91568850695171, -0.9689944594115154, 3.0438037242978453, -24.495224566215796,
-     20.176138334709044, 15.98066361424651, -6.789040303419874, -6.710236069923372},
-    {11.419903575922262, 2.8879645146136994, 72.92137995996029, 80.12511834622643,
-     -52.072871366152654, -59.78993625266729, -0.15582684282751913, 4.883087185713722},
-};
-  return t[r][m];
-}
-constexpr double FACTOR_MIN = 0.2;
-constexpr double FACTOR_MAX = 6.0;
 
 typedef MDX_LU_T lu_t;
 // The stage increments are rounded to the LU type when stored (the reference's

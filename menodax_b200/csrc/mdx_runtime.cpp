@@ -176,6 +176,13 @@ int load_for_context(mdx_plan* plan, Loaded** out) {
     if ((r = g_driver.moduleGetFunction(&l.grad, l.module, "mdx_grad_reverse")) != CUDA_SUCCESS)
       return cuda_fail(r, "cuModuleGetFunction(mdx_grad_reverse)");
   }
+  // Above the 48 KB default a kernel's dynamic shared memory has to be opted into.
+  if (plan->desc.shared_bytes > 48 * 1024) {
+    for (CUfunction f : {l.plain, l.persistent}) {
+      r = g_driver.funcSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, plan->desc.shared_bytes);
+      if (r != CUDA_SUCCESS) return cuda_fail(r, "cuFuncSetAttribute(MAX_DYNAMIC_SHARED_SIZE_BYTES)");
+    }
+  }
   CUdevice dev;
   if ((r = g_driver.ctxGetDevice(&dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
   if ((r = g_driver.deviceGetAttribute(&l.sm_count, CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT, dev)) != CUDA_SUCCESS)
@@ -258,6 +265,13 @@ int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
   if (!desc->cubin || desc->cubin_size == 0) return fail(MDX_E_INVALID, "mdx_plan_create: empty cubin");
   if ((desc->flags & MDX_PLAN_CHECKPOINT) && desc->ckpt_stride < 1)
     return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt_stride >= 1; got %d", desc->ckpt_stride);
+  const int team = desc->team_size;
+  if (team != 1 && team != 4 && team != 8 && team != 16 && team != 32)
+    return fail(MDX_E_INVALID, "team_size must be 1, 4, 8, 16 or 32; got %d", team);
+  if (team > 1 && (desc->flags & (MDX_PLAN_CHECKPOINT | MDX_PLAN_ADJOINT | MDX_PLAN_SAVE_HOOK)))
+    return fail(MDX_E_INVALID, "a team module (team_size %d) has no checkpoint, adjoint or save-hook kernels", team);
+  if (desc->shared_bytes < 0 || desc->shared_bytes > MDX_MAX_SHARED_BYTES)
+    return fail(MDX_E_INVALID, "shared_bytes must be in [0, %d]; got %d", MDX_MAX_SHARED_BYTES, desc->shared_bytes);
   mdx_plan* p = new (std::nothrow) mdx_plan;
   if (!p) return fail(MDX_E_NOMEM, "out of host memory");
   p->desc = *desc;
@@ -301,7 +315,7 @@ int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count) {
   int rc = load_for_context(plan, &l);
   if (rc) return rc;
   CUfunction f = mode == MDX_LAUNCH_PERSISTENT ? l->persistent : l->plain;
-  CUresult r = g_driver.occupancy(blocks_per_sm, f, plan->desc.threads_per_block, 0);
+  CUresult r = g_driver.occupancy(blocks_per_sm, f, plan->desc.threads_per_block, (size_t)plan->desc.shared_bytes);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
   *sm_count = l->sm_count;
   return MDX_OK;
@@ -365,31 +379,34 @@ int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, in
   a.atol = d->atol;
 
   const unsigned tpb = (unsigned)plan->desc.threads_per_block;
+  const unsigned smem = (unsigned)plan->desc.shared_bytes;
+  // Trajectories per block: one per thread, or one per team of team_size lanes.
+  const int per_block = (int)tpb / plan->desc.team_size;
   CUstream s = (CUstream)stream;
   CUfunction f;
   unsigned grid;
   if (d->mode == MDX_LAUNCH_PLAIN) {
     f = l->plain;
-    grid = (unsigned)((d->n_traj + tpb - 1) / tpb);
+    grid = (unsigned)((d->n_traj + per_block - 1) / per_block);
   } else {
     f = l->persistent;
     a.work_counter = counter ? counter : (int*)d->workspace;
     int blocks = d->grid_blocks;
     if (blocks <= 0) {
       int per_sm = 0;
-      CUresult r = g_driver.occupancy(&per_sm, f, (int)tpb, 0);
+      CUresult r = g_driver.occupancy(&per_sm, f, (int)tpb, (size_t)smem);
       if (r != CUDA_SUCCESS) return cuda_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
       if (per_sm < 1) per_sm = 1;
       blocks = per_sm * l->sm_count;
     }
-    const int needed = (d->n_traj + (int)tpb - 1) / (int)tpb;
+    const int needed = (d->n_traj + per_block - 1) / per_block;
     if (blocks > needed) blocks = needed;
     grid = (unsigned)blocks;
     CUresult r = g_driver.memsetD32Async((CUdeviceptr)a.work_counter, 0u, 1, s);
     if (r != CUDA_SUCCESS) return cuda_fail(r, "cuMemsetD32Async(work counter)");
   }
   void* params[] = {&a};
-  CUresult r = g_driver.launchKernel(f, grid, 1, 1, tpb, 1, 1, 0, s, params, nullptr);
+  CUresult r = g_driver.launchKernel(f, grid, 1, 1, tpb, 1, 1, smem, s, params, nullptr);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_solve)");
   return MDX_OK;
 }

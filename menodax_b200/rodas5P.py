@@ -4,16 +4,21 @@ Same signature and defaults as ``modax/rodas5P.py:1024-1051``, same errors
 (``modax/rodas5P.py:1204-1211``), same outputs: ``hist (N, S, n_vars)`` or
 ``(hist, stats)``.  Extra keyword ``launch`` picks the one-launch kernel
 (``"plain"``), the persistent refill kernel (``"persistent"``) or lets the
-library choose (``"auto"``).
+library choose (``"auto"``); ``team`` picks one thread or a team of lanes per
+trajectory.
 """
 
 from __future__ import annotations
 
+from dataclasses import replace
+
+import numpy as np
 import torch
 
 from menodax_b200._frontend import run
-from menodax_b200._problem import KernelOptions
+from menodax_b200._problem import KernelOptions, team_block_threads
 from menodax_b200._sparsity import normalize_sparsity
+from menodax_b200._team import TEAM_SIZES
 
 _DEFAULT_TRAJECTORIES_PER_BLOCK = 32
 LU_PRECISIONS = ("fp32", "fp64")
@@ -64,6 +69,7 @@ def solve(
     launch: str = "auto",
     sparse_code: str = "auto",
     arithmetic: str = "auto",
+    team="auto",
 ):
     """Rodas5P ensemble solve of ``y' = ode_fn(y, t, p)`` on one GPU.
 
@@ -78,6 +84,14 @@ def solve(
     ``(nnz, 2)`` pairs) colours the Jacobian sweep and compiles a sparse LU for the
     pattern, ordered by ``ordering`` (``"amd"`` or ``"natural"``).  ``tf_index``
     names a parameter column holding each trajectory's own end time.
+
+    ``team`` picks the kernel layout: ``0`` runs one trajectory per thread with
+    its vectors and matrix in registers (the reference's layout); ``4``, ``8``,
+    ``16`` or ``32`` give each trajectory a team of that many lanes with its
+    vectors and matrix in shared memory; ``"auto"`` leaves the choice to the
+    launch autotuner, which considers teams for systems of
+    ``autotune.TEAM_MIN_VARS`` or more states.  Teams run the plain system only
+    (no save hook, sensitivities or gradients).
 
     ``save_hook(save_idx, y, t, p_row, acc)`` runs inside the kernel at every save
     (the initial state, each dense-output save, the frozen saves past a
@@ -108,6 +122,7 @@ def solve(
     elif not save_history:
         raise ValueError("save_history=False needs a save_hook to consume the saves")
     n_vars = int(torch.as_tensor(y0).shape[-1]) if not hasattr(y0, "shape") else int(y0.shape[-1])
+    team_choice = _team_option(team)
     if sparsity is not None:
         sparsity = normalize_sparsity(sparsity, n_vars)
     tpb = trajectories_per_block_or_default(trajectories_per_block)
@@ -130,7 +145,14 @@ def solve(
     )
     from menodax_b200.autograd import needs_grad, solve_with_grad
 
-    if needs_grad(y0, params):
+    grad = needs_grad(y0, params)
+    if team_choice:
+        if save_hook is not None or grad:
+            raise ValueError("a team kernel solves the plain system: no save_hook and no gradients")
+        options = replace(options, team=team_choice)
+        options = replace(options, threads_per_block=team_block_size(
+            team_choice, trajectories_per_block, n_vars, _n_params(params), options))
+    if grad:
         if save_hook is not None:
             raise NotImplementedError("a solve with a save_hook is not differentiable")
         return solve_with_grad(
@@ -141,4 +163,33 @@ def solve(
         ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
         max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
         launch_mode=launch, tune_block=trajectories_per_block is None,
+        tune_team=team == "auto" and save_hook is None,
     )
+
+
+def _team_option(team) -> int:
+    if team == "auto":
+        return 0
+    if team in (0, None):
+        return 0
+    if team not in TEAM_SIZES:
+        raise ValueError(f"team must be 'auto', 0 or one of {TEAM_SIZES}; got {team!r}")
+    return int(team)
+
+
+def _n_params(params) -> int:
+    shape = params.shape if hasattr(params, "shape") else np.shape(params)
+    return int(shape[-1]) if len(shape) else 1
+
+
+def team_block_size(team: int, trajectories_per_block, n_vars: int, n_params: int, options) -> int:
+    """Threads per block of a team launch: ``trajectories_per_block`` teams, by default
+    up to 128 threads as the block's shared memory allows."""
+    if trajectories_per_block is None:
+        return team_block_threads(n_vars, n_params, options)
+    threads = int(trajectories_per_block) * team
+    if threads % 32 or threads > 1024:
+        raise ValueError(
+            f"trajectories_per_block={trajectories_per_block} with team={team} gives {threads} threads; "
+            "a block must be whole warps, at most 1024 threads")
+    return threads

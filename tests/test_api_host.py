@@ -44,3 +44,18 @@ def test_normalisation_broadcasts():
 def test_trajectories_per_block_default():
     assert rodas5P.trajectories_per_block_or_default() == 32
     assert rodas5P.trajectories_per_block_or_default(8) == 8
+
+
+def test_team_option_errors():
+    cfg = systems.vdp_ring_config(4, size=4)
+    args = (cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"])
+    with pytest.raises(ValueError, match="team must be"):
+        rodas5P.solve(*args, team=3)
+
+    def hook(save_idx, y, t, p, acc):
+        acc[0] = acc[0] + y[0]
+
+    with pytest.raises(ValueError, match="save_hook"):
+        rodas5P.solve(*args, team=8, save_hook=hook, hook_size=1)
+    with pytest.raises(ValueError, match="whole warps"):
+        rodas5P.solve(*args, team=8, trajectories_per_block=3)

@@ -124,8 +124,10 @@ __device__ __forceinline__ void factorize(Slice& s, const Lanes& L) {
 #endif
 }
 
-// Solve M x = x in place on stage row x.
-__device__ __forceinline__ void solve(Slice& s, lu_t* x, const Lanes& L) {
+// Solve M x = x in place on stage row x.  One copy serves the eight stages: the
+// substitutions are the largest straight-line code of a step, and eight inlined
+// copies overflow the instruction cache (ncu: "no instruction" stalls).
+__device__ __noinline__ void solve(Slice& s, lu_t* x, const Lanes L) {
 #if MDX_TEAM_DENSE
   dense_solve<MDX_NV, MDX_TEAM_LDA, lu_t, MDX_FAST != 0>(s.lu, s.perm, x, L.lane, L.mask);
 #else

@@ -11,6 +11,7 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import os
+import re
 import subprocess
 import threading
 from pathlib import Path
@@ -165,27 +166,40 @@ def check(rc: int, what: str):
         raise NativeError(f"{what} failed ({rc}): {last_error()}")
 
 
-def _kernel_header_digest() -> str:
-    h = hashlib.sha256()
-    for f in sorted(KERNEL_DIR.glob("*")):
-        if f.is_file():
-            h.update(f.name.encode())
-            h.update(f.read_bytes())
-    return h.hexdigest()
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.MULTILINE)
+_header_text: dict[str, bytes] = {}
 
 
-_header_digest = None
+def _included_headers(source: str) -> list[str]:
+    """The kernel headers ``source`` includes, directly or through other headers, sorted."""
+    seen: set[str] = set()
+    todo = _INCLUDE.findall(source)
+    while todo:
+        name = todo.pop()
+        if name in seen:
+            continue
+        path = KERNEL_DIR / name
+        if not path.is_file():
+            continue
+        seen.add(name)
+        if name not in _header_text:
+            _header_text[name] = path.read_bytes()
+        todo.extend(_INCLUDE.findall(_header_text[name].decode()))
+    return sorted(seen)
 
 
 def compile_cubin(source: str, options: list[str], name: str = "mdx_problem.cu") -> bytes:
-    """NVRTC-compile ``source`` for sm_100a, through an on-disk cache keyed on its text."""
-    global _header_digest
-    if _header_digest is None:
-        _header_digest = _kernel_header_digest()
+    """NVRTC-compile ``source`` for sm_100a, through an on-disk cache keyed on its
+    text, the text of every kernel header it includes, and the options."""
     opts = [f"-I{KERNEL_DIR}", "-arch=sm_100a", "-std=c++17", "-default-device", "-lineinfo"] + list(options)
-    key = hashlib.sha256(
-        "\0".join([source, _header_digest, *opts]).encode()
-    ).hexdigest()
+    h = hashlib.sha256()
+    for part in (source, *opts):
+        h.update(part.encode())
+        h.update(b"\0")
+    for header in _included_headers(source):
+        h.update(header.encode())
+        h.update(_header_text[header])
+    key = h.hexdigest()
     cache_dir = Path(os.environ.get("MENODAX_CUBIN_CACHE", CUBIN_CACHE))
     path = cache_dir / f"{key}.cubin"
     if path.exists():

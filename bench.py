@@ -375,6 +375,8 @@ def run_config(args):
             hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
         barrier(world)
         ms = []
+        # NVTX range per variant: ncu --nvtx --nvtx-include "timed:<variant>/" takes its launches.
+        torch.cuda.nvtx.range_push(f"timed:{name}")
         for _ in range(args.steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -382,6 +384,7 @@ def run_config(args):
             hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
             e1.record(stream)
             ms.append((e0, e1))
+        torch.cuda.nvtx.range_pop()
         barrier(world)
         t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
         results[name] = {"solves_per_s": n * world * args.steps / (t * 1e-3), "ms_per_solve": t / args.steps,
@@ -489,7 +492,11 @@ def main():
         sampler.start()
         time.sleep(0.3)
     if args.profile:
+        # The timed launches sit in an NVTX range "timed", so a capture can take
+        # exactly them: ncu --nvtx --nvtx-include "timed/" ...
+        torch.cuda.nvtx.range_push("timed")
         timed(tuned, choice.mode, args.steps, args.warmup, tuned_grid)
+        torch.cuda.nvtx.range_pop()
         print(json.dumps({"profile": "done", "launch": choice.describe()}))
         return
     ms = timed(tuned, choice.mode, args.steps, args.warmup, tuned_grid)

@@ -18,14 +18,14 @@ LU, and for dense LUs only while the matrix stays in registers
 (``DENSE_UNROLL_MAX``): past that its matrix lives in local memory and a team is
 faster by an order of magnitude.
 
-Tuning is bounded in time.  The first candidate runs on the leading ``PROBE``
-trajectories with at most ``PROBE_STEPS`` steps each.  When that finishes every
-trajectory, its time bounds a launch, and the candidates are timed on the whole
-ensemble, or on the probe set when that would exceed ``BUDGET_S``.  When it hits
-the step cap the integrations are long (tens of thousands of steps): the plain
-candidates are ranked by the capped probe, which measures the cost of a step
-with the device full, and the winner runs as a persistent refill launch, since
-long stiff ensembles have uneven step counts.
+Tuning is bounded in time.  The first candidate runs on the whole ensemble
+with at most ``PROBE_STEPS`` steps per trajectory.  When that finishes every
+trajectory, its time is a launch's, and the candidates are timed in full, or on
+the leading ``PROBE`` trajectories when that would exceed ``BUDGET_S``.  When it
+hits the step cap the integrations are long (tens of thousands of steps): the
+plain candidates are ranked by the same capped run, which measures the cost of
+a step with the ensemble resident, and the winner runs as a persistent refill
+launch, since long stiff ensembles have uneven step counts.
 """
 
 from __future__ import annotations
@@ -119,13 +119,14 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
     kernel is a candidate too (for systems of ``TEAM_MIN_VARS`` states or more);
     an ``options.team`` already set is kept and only its launch kind is tuned.
 
-    The first candidate runs once on the leading ``PROBE`` trajectories with at
-    most ``PROBE_STEPS`` steps each.  If that finished every trajectory, its time
-    bounds a launch and the candidates are timed on the whole ensemble (or on
-    the probe set, to stay within ``BUDGET_S``).  If it hit the step cap, the
-    integrations are long: the plain launches are ranked by the same capped
-    probe -- the cost per step with the device full -- and the winner runs as a
-    persistent launch, which refills lanes as the uneven trajectories finish."""
+    The first candidate runs once on the whole ensemble with at most
+    ``PROBE_STEPS`` steps per trajectory.  If that finished every trajectory, its
+    time is a launch's, and the candidates are timed in full (on the leading
+    ``PROBE`` trajectories when that would exceed ``BUDGET_S``).  If it hit the
+    step cap, the integrations are long: the plain launches are ranked by the
+    same capped run -- the cost of a step with the ensemble resident -- and the
+    winner runs as a persistent launch, which refills lanes as the uneven
+    trajectories finish."""
     n = y0.shape[0]
     if options.team:
         blocks, teams = (), ((options.team, options.threads_per_block),)
@@ -168,10 +169,8 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
                   n_save_hist=n_save_hist)
     m = min(n, PROBE)
     cap = min(int(max_steps), PROBE_STEPS)
-    first = buildable[0]
-    probe_s, counters = _timed_launch(problem_for(replace(first, mode=_native.MDX_LAUNCH_PLAIN, grid_fill=0.0)),
-                                      replace(first, mode=_native.MDX_LAUNCH_PLAIN, grid_fill=0.0), stream,
-                                      n=m, max_steps=cap, **inputs)
+    first = replace(buildable[0], mode=_native.MDX_LAUNCH_PLAIN, grid_fill=0.0)
+    probe_s, counters = _timed_launch(problem_for(first), first, stream, n=n, max_steps=cap, **inputs)
     capped = cap < int(max_steps) and int(counters[2].max()) >= cap
     if capped:
         best = None
@@ -179,8 +178,8 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
             if choice.mode != _native.MDX_LAUNCH_PLAIN:
                 continue
             prob = problem_for(choice)
-            _timed_launch(prob, choice, stream, n=m, max_steps=cap, **inputs)
-            secs, _ = _timed_launch(prob, choice, stream, n=m, max_steps=cap, **inputs)
+            _timed_launch(prob, choice, stream, n=n, max_steps=cap, **inputs)
+            secs, _ = _timed_launch(prob, choice, stream, n=n, max_steps=cap, **inputs)
             if best is None or secs < best[0]:
                 best = (secs, choice)
         winner = best[1]

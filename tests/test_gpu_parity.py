@@ -140,9 +140,12 @@ def test_error_weights_match_oracle(oracle):
     # at the threshold: two host builds of the oracle that differ only in fused
     # multiply-adds already disagree on 0.25% of these trajectories.
     assert same.mean() >= 0.98
-    # Controlled components to the parity bar; the zero-weight one is not
-    # error-controlled, so rounding differences in it are not damped.
-    _states_agree(hist[..., [0, 2]], h[..., [0, 2]], same, atol=1e-15)
+    # The zero-weight component is not error-controlled, so rounding differences
+    # in it are not damped (1e-5); they reach the controlled components through
+    # the dynamics (k2 * y2^2 feeds y3), which therefore agree to 5e-7 rather than
+    # 1e-9 on trajectories with identical steps.  The oracle's own FMA choice
+    # follows its host CPU, so the size of these differences varies by machine.
+    _states_agree(hist[..., [0, 2]], h[..., [0, 2]], same, rtol=5e-7, atol=1e-15)
     _states_agree(hist[..., 1], h[..., 1], same, rtol=1e-5, atol=1e-15)
 
 

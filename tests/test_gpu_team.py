@@ -7,6 +7,8 @@ oracle with FP32 LUs.  The persistent team launch must reproduce the plain one
 bit for bit (the queue only changes which team runs a trajectory).
 """
 
+import math
+
 import numpy as np
 import pytest
 
@@ -85,3 +87,52 @@ def test_team_stats_and_max_steps_status():
                              sparsity=cfg["sparsity"], team=8, max_steps=50, return_stats=True)
     assert (np.asarray(stats["loop_steps"]) == 50).all()
     assert (np.asarray(stats["status"]) & 1).all()
+
+
+def test_team_tf_index_and_time_derivative():
+    """The reference's tests/test_solver_options.py:40-93 cases on the team kernel:
+    df/dt reaches the stages of a non-autonomous system, and tf_index ends each
+    trajectory at its own time with the later saves frozen."""
+    t_span = np.linspace(0.0, 1.0, 11)
+    params = np.array([[10.0, 5.0, 1.0], [10.0, 5.0, 0.5]])
+    out = rodas5P.solve(systems.forced_decay, np.zeros((2, 1)), t_span, params, tf_index=2, rtol=1e-10,
+                        atol=1e-12, first_step=1e-4, lu_precision="fp64", team=4)
+    exact = 5.0 * (10.0 * t_span - 1.0 + np.exp(-10.0 * t_span)) / 100.0
+    np.testing.assert_allclose(out[0, :, 0], exact, rtol=1e-8, atol=1e-10)
+    stops = int(np.searchsorted(t_span, 0.5, side="right"))
+    np.testing.assert_allclose(out[1, :stops, 0], exact[:stops], rtol=1e-8, atol=1e-10)
+    assert (out[1, stops:, 0] == out[1, stops - 1, 0]).all()
+
+
+def _forced_ring(y, t, p):
+    n = 12
+    return tuple(-p[0] * y[i] + 0.3 * (y[(i + 1) % n] - y[i]) + math.sin(t + 0.5 * i) for i in range(n))
+
+
+@pytest.mark.parametrize("layout", ["sparse", "dense"])
+def test_team_non_autonomous_ring_matches_thread_kernel(layout):
+    n = 12
+    rng = np.random.default_rng(11)
+    y0 = rng.uniform(-1.0, 1.0, size=(300, n))
+    p = rng.uniform(0.5, 2.0, size=(300, 1))
+    t_span = np.linspace(0.0, 5.0, 9)
+    pattern = [(i, i) for i in range(n)] + [(i, (i + 1) % n) for i in range(n)] if layout == "sparse" else None
+    kw = dict(rtol=1e-9, atol=1e-11, lu_precision="fp64", sparsity=pattern, return_stats=True)
+    h0, s0 = rodas5P.solve(_forced_ring, y0, t_span, p, team=0, **kw)
+    h8, s8 = rodas5P.solve(_forced_ring, y0, t_span, p, team=8, **kw)
+    same = np.asarray(s0["loop_steps"]) == np.asarray(s8["loop_steps"])
+    assert same.mean() >= 0.999
+    np.testing.assert_allclose(h8[same], h0[same], rtol=1e-9, atol=1e-12)
+
+
+def test_team_error_weights_match_thread_kernel():
+    cfg = systems.robertson_config(size=256)
+    w = np.array([1.0, 0.0, 1.0])
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64", error_weights=w, return_stats=True)
+    h0, s0 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], team=0, **kw)
+    h4, s4 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], team=4, **kw)
+    same = np.asarray(s0["loop_steps"]) == np.asarray(s4["loop_steps"])
+    assert same.mean() >= 0.98
+    # As against the oracle: the zero-weight component's undamped rounding
+    # differences reach the controlled ones through the dynamics.
+    np.testing.assert_allclose(h4[same][..., [0, 2]], h0[same][..., [0, 2]], rtol=5e-7, atol=1e-15)

@@ -129,6 +129,10 @@ typedef struct mdx_grad_desc {
   double* grad_y0;         /* (n_traj, n_vars), overwritten */
   double* grad_params;     /* (n_traj, n_params), overwritten */
   int* status;             /* (n_traj,) or NULL */
+  const int* order;        /* (n_traj,) or NULL: a permutation of 0..n_traj-1, the order in
+                              which trajectories are handed to threads -- e.g. longest first by
+                              ckpt_count, so the longest reverse sweeps start in the first
+                              wave of resident blocks */
 } mdx_grad_desc;
 
 /* NVRTC: compile CUDA C++ `source` to an sm_100a cubin.  Needs no GPU.

@@ -82,6 +82,7 @@ class GradDesc(ctypes.Structure):
         ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p),
         ("ckpt_capacity", ctypes.c_longlong), ("grad_hist", ctypes.c_void_p),
         ("grad_y0", ctypes.c_void_p), ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p),
+        ("order", ctypes.c_void_p),
     ]
 
 

@@ -115,6 +115,11 @@ class _EnsembleSolve(torch.autograd.Function):
         d.grad_y0 = grad_y0.data_ptr()
         d.grad_params = grad_p.data_ptr()
         d.status = status.data_ptr()
+        # Longest reverse sweeps first: the reverse kernel's registers leave room
+        # for only part of a large ensemble at once, and a long trajectory that
+        # started in a later wave would set the makespan.
+        order = torch.argsort(ckpt_count, descending=True, stable=True).to(torch.int32)
+        d.order = order.data_ptr()
         stream = torch.cuda.current_stream(params.device).cuda_stream
         with torch.cuda.device(params.device):
             problem.plan.grad(d, stream)

@@ -363,8 +363,9 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 // frozen saves); save 0 is y0 itself.
 extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
 mdx_grad_reverse(const MdxGradArgs a) {
-  const int traj = blockIdx.x * blockDim.x + threadIdx.x;
-  if (traj >= a.n_traj) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_traj) return;
+  const int traj = a.order ? a.order[i] : i;
   double p[MDX_NP > 0 ? MDX_NP : 1];
 #pragma unroll
   for (int k = 0; k < MDX_NP; ++k) p[k] = a.params[(size_t)traj * MDX_NP + k];

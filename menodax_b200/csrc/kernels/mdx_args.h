@@ -50,6 +50,7 @@ typedef struct MdxGradArgs {
   double* grad_y0;         /* (N, n_vars) */
   double* grad_params;     /* (N, n_params) */
   int* status;             /* may be NULL */
+  const int* order;        /* may be NULL: thread i takes trajectory order[i] */
   long long ckpt_capacity;
   int n_traj;
   int n_save;

@@ -461,6 +461,7 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
   a.grad_y0 = d->grad_y0;
   a.grad_params = d->grad_params;
   a.status = d->status;
+  a.order = d->order;
   a.ckpt_capacity = d->ckpt_capacity;
   a.n_traj = d->n_traj;
   a.n_save = d->n_save;

@@ -1,10 +1,11 @@
 """torch.autograd front end: the discrete adjoint of an ensemble solve.
 
 ``rodas5P.solve`` / ``tsit5.solve`` route here when a torch input requires
-grad.  The forward pass runs the checkpointing kernel, which records one
-``(t, h, y)`` step state per accepted step; ``backward`` launches the reverse
-kernel (``mdx_grad`` in the C ABI), which replays every accepted step from its
-state and returns the cotangents of ``y0`` and ``params``.  Step sizes are
+grad.  The forward pass runs the checkpointing kernel, which records every
+accepted step's size and the start state ``(t, y)`` of every K-th step;
+``backward`` launches the reverse kernel (``mdx_grad`` in the C ABI), which
+replays each K-step segment from its start state, reverses it step by step and
+returns the cotangents of ``y0`` and ``params``.  Step sizes are
 constants of the discrete map, so the gradient is the exact derivative of the
 solution the forward pass produced -- for that step sequence it equals what the
 reference's forward sensitivities give with ``sens_error_control=False``

@@ -1,0 +1,126 @@
+"""The launch autotuner's decisions, with the timed launches replaced by a cost table.
+
+No GPU: ``autotune._timed_launch`` and ``get_problem`` are stand-ins, so what is
+checked is which candidates exist for which systems, which path the step-capped
+probe takes, and which launch comes back.
+"""
+
+from types import SimpleNamespace
+
+import pytest
+import torch
+
+from menodax_b200 import _native, autotune, systems
+from menodax_b200._problem import KernelOptions
+from menodax_b200._sparsity import normalize_sparsity
+
+PLAIN, PERSISTENT = _native.MDX_LAUNCH_PLAIN, _native.MDX_LAUNCH_PERSISTENT
+
+
+class Recorder:
+    """Fake timed launch: seconds from ``cost(choice, n, max_steps)``, steps from ``steps``."""
+
+    def __init__(self, cost, steps):
+        self.cost = cost
+        self.steps = steps
+        self.calls = []
+
+    def __call__(self, problem, choice, stream, *, n, max_steps, **_):
+        self.calls.append((choice, n, max_steps))
+        counters = torch.zeros((4, n), dtype=torch.int32)
+        counters[2] = min(self.steps, max_steps)
+        return self.cost(choice, n, max_steps), counters
+
+
+@pytest.fixture
+def fake_device(monkeypatch):
+    plan = SimpleNamespace(occupancy=lambda mode: (4, 148))
+    monkeypatch.setattr(autotune, "get_problem", lambda *a, **k: SimpleNamespace(plan=plan))
+    monkeypatch.setattr(torch.cuda, "current_stream", lambda *a, **k: None)
+    monkeypatch.setattr(torch.cuda, "get_device_name", lambda *a, **k: "fake B200")
+    autotune._cache.clear()
+    yield
+    autotune._cache.clear()
+
+
+def _tune(fn, n_vars, options, recorder, monkeypatch, n=8192, max_steps=100000, **kw):
+    monkeypatch.setattr(autotune, "_timed_launch", recorder)
+    y0 = torch.zeros((n, n_vars), dtype=torch.float64)
+    params = torch.zeros((n, 1), dtype=torch.float64)
+    return autotune.tune(fn, n_vars, 1, options, y0=y0, times=torch.zeros(3, dtype=torch.float64),
+                         params=params, weights=None, dt0=0.0, rtol=1e-6, atol=1e-8,
+                         max_steps=max_steps, **kw)
+
+
+def _ring(n_osc):
+    fn, _ = systems.make_vdp_system(n_osc, mu=1.0, d=0.1)
+    return fn, 2 * n_osc, normalize_sparsity(systems.vdp_sparsity(n_osc), 2 * n_osc)
+
+
+def test_short_integrations_time_every_candidate_and_keep_the_fastest(fake_device, monkeypatch):
+    fn, n, pattern = _ring(16)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern)
+
+    def cost(choice, n_traj, steps):
+        return 0.010 if (choice.team == 16 and choice.mode == PERSISTENT) else 0.020
+
+    rec = Recorder(cost, steps=120)
+    choice = _tune(fn, n, opts, rec, monkeypatch, tune_team=True)
+    assert (choice.team, choice.mode) == (16, PERSISTENT)
+    timed = {(c.team, c.mode, c.threads_per_block, c.grid_fill) for c, _, s in rec.calls if s == 100000}
+    # thread launches at three block sizes (plain + two fills) and two launch kinds per team size
+    assert len(timed) == 3 * 3 + 2 * len(autotune.team_sizes_for(n))
+
+
+def test_long_integrations_rank_plain_launches_by_a_capped_run(fake_device, monkeypatch):
+    fn, n, pattern = _ring(64)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern)
+
+    def cost(choice, n_traj, steps):
+        return 1.0 if choice.team == 8 else 2.0
+
+    rec = Recorder(cost, steps=100000)
+    choice = _tune(fn, n, opts, rec, monkeypatch, tune_team=True)
+    assert choice.team == 8 and choice.mode == PERSISTENT and choice.grid_fill == 1.0
+    # every launch was capped, ran the whole ensemble, and only plain launches were ranked
+    assert all(s == autotune.PROBE_STEPS and m == 8192 for _, m, s in rec.calls)
+    assert all(c.mode == PLAIN for c, _, _ in rec.calls)
+
+
+def test_long_integrations_pick_the_half_filled_persistent_thread_launch(fake_device, monkeypatch):
+    fn, n, pattern = _ring(4)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern)
+
+    def cost(choice, n_traj, steps):
+        return 1.0 if choice.threads_per_block == 64 else 2.0
+
+    choice = _tune(fn, n, opts, Recorder(cost, steps=100000), monkeypatch, tune_team=True)
+    assert (choice.team, choice.threads_per_block, choice.mode, choice.grid_fill) == (0, 64, PERSISTENT, 0.5)
+
+
+def test_candidate_families_follow_the_system_size(fake_device, monkeypatch):
+    seen = {}
+
+    def run(key, fn, n, opts):
+        rec = Recorder(lambda c, m, s: 1.0, steps=10)
+        _tune(fn, n, opts, rec, monkeypatch, tune_team=True)
+        seen[key] = {c.team for c, _, _ in rec.calls}
+
+    fn, n, pattern = _ring(4)
+    run("ring8 sparse", fn, n, KernelOptions(sparsity=pattern))
+    run("ring8 dense", fn, n, KernelOptions())
+    fn, n, pattern = _ring(32)
+    run("ring64 sparse", fn, n, KernelOptions(sparsity=pattern, fast=True))
+    run("ring64 dense", fn, n, KernelOptions(fast=True))
+    assert seen["ring8 sparse"] == {0} and seen["ring8 dense"] == {0}   # below TEAM_MIN_VARS
+    assert 0 in seen["ring64 sparse"] and seen["ring64 sparse"] - {0}   # sparse: threads and teams
+    assert 0 not in seen["ring64 dense"]                                # dense past registers: teams only
+
+
+def test_a_fixed_team_is_only_tuned_for_its_launch_kind(fake_device, monkeypatch):
+    fn, n, pattern = _ring(16)
+    opts = KernelOptions(sparsity=pattern, team=8, threads_per_block=128)
+    rec = Recorder(lambda c, m, s: 1.0 if c.mode == PLAIN else 0.5, steps=10)
+    choice = _tune(fn, n, opts, rec, monkeypatch)
+    assert {c.team for c, _, _ in rec.calls} == {8}
+    assert (choice.team, choice.threads_per_block, choice.mode) == (8, 128, PERSISTENT)

@@ -23,8 +23,8 @@ from menodax_b200 import _native
 from menodax_b200._ensemble import initial_step, launch, pick_device, solver_stats
 from menodax_b200._problem import get_problem
 
-# Checkpoint capacity (accepted steps per trajectory) last seen per problem, so a
-# repeated gradient call sizes its buffer without a counting pass.
+# Checkpoint capacity (accepted steps per trajectory) and stride last used per
+# problem, so a repeated gradient call sizes its buffer without a counting pass.
 _capacity_hint: dict = {}
 
 # Steps per recorded start state.  One record per step costs (n + 2) doubles a
@@ -41,6 +41,11 @@ def checkpoint_bytes(n_traj, n_vars, capacity, stride):
 
 def choose_stride(n_traj, n_vars, capacity, device):
     free, _ = torch.cuda.mem_get_info(device)
+    # Memory torch's caching allocator holds for no live tensor -- the previous
+    # call's checkpoint buffer, typically -- is free for this one too; leaving it
+    # out would pick a coarser stride on every call after the first, and a
+    # stride is a separately compiled kernel.
+    free += torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
     budget = MEMORY_FRACTION * free
     for stride in CKPT_STRIDES:
         if checkpoint_bytes(n_traj, n_vars, capacity, stride) <= budget:
@@ -70,13 +75,17 @@ class _EnsembleSolve(torch.autograd.Function):
         pc = params.detach().contiguous()
         kw = dict(y0=y0c, times=times, params=pc, weights=None, dt0=dt0, rtol=rtol, atol=atol,
                   max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN)
-        capacity = _capacity_hint.get(key)
+        capacity, stride_hint = _capacity_hint.get(key, (None, None))
         if capacity is None:
             # First call for this problem: count the accepted steps with a plain solve.
             _, counters = launch(problems["plain"], **kw)
             capacity = max(1, int(counters[0].max().item()) if n else 1)
         while True:
             stride = choose_stride(n, problems["plain"].n_vars, capacity, y0.device)
+            # Keep the last call's stride when memory still allows it: the same
+            # compiled kernel and the same replay cost from call to call.
+            if stride_hint is not None and stride < stride_hint:
+                stride = stride_hint
             problem = problems[stride]
             nbytes = problem.plan.checkpoint_size(n, capacity)
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
@@ -87,7 +96,7 @@ class _EnsembleSolve(torch.autograd.Function):
                 break
             capacity = int(needed * 1.1) + 8
             del ckpt
-        _capacity_hint[key] = max(needed + 8, int(needed * 1.1))
+        _capacity_hint[key] = (max(needed + 8, int(needed * 1.1)), stride)
         ctx.problem = problem
         ctx.capacity = capacity
         ctx.save_for_backward(pc, times, ckpt, ckpt_count)

@@ -295,6 +295,32 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
 
 
 # --------------------------------------------------------------------------- other configurations
+def config_roofline(fn, n_vars, n_params, opts, counters, n, n_save, launch_ms, peaks):
+    """Algorithmic FP64 + LU-type operations of one launch (attempted steps the
+    kernel reported x per-step counts of the traced problem) over its device
+    time, against the measured CUDA-core peaks blended by the same mix."""
+    import torch
+
+    from menodax_b200._flops import rodas5p_cost, tsit5_cost
+    from menodax_b200._sparse_direct import sparse_direct_solver_for
+
+    if opts.solver == "tsit5":
+        cost = tsit5_cost(fn, n_vars, n_params)
+    else:
+        sparse = sparse_direct_solver_for(opts.sparsity, opts.ordering) if opts.sparsity is not None else None
+        cost = rodas5p_cost(fn, n_vars, n_params, sparse=sparse)
+    steps = float(counters[2].to(torch.float64).sum())
+    f64 = steps * cost.f64 + n * (n_save - 1) * cost.per_save
+    lu = steps * cost.lu
+    peak64, peak32 = peaks
+    lu_peak = peak32 if opts.lu_precision == "fp32" else peak64
+    seconds = launch_ms * 1e-3
+    t_roof = f64 / peak64 + lu / lu_peak
+    achieved = (f64 + lu) / seconds
+    return {"bound": "fp64", "achieved": achieved / 1e12, "peak": (f64 + lu) / t_roof / 1e12,
+            "unit": "TFLOP/s", "frac": t_roof / seconds}
+
+
 def run_config(args):
     """One line per non-headline configuration: device-timed solves/s of the
     autotuned FP32-LU kernel (Tsit5: FP64) and of the plain FP64 reference-
@@ -359,6 +385,7 @@ def run_config(args):
     stream = torch.cuda.current_stream(dev)
     results = {}
     stats = None
+    peaks = (_native.measure_fma_peak(True), _native.measure_fma_peak(False))
     for name, opts in variants:
         if name.startswith("plain"):
             prob, mode, grid = get_problem(fn, n_vars, n_params, opts), _native.MDX_LAUNCH_PLAIN, 0
@@ -388,7 +415,9 @@ def run_config(args):
         barrier(world)
         t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
         results[name] = {"solves_per_s": n * world * args.steps / (t * 1e-3), "ms_per_solve": t / args.steps,
-                         "launch": label}
+                         "launch": label,
+                         "roofline": config_roofline(fn, n_vars, n_params, opts, counters, n,
+                                                     times.numel(), t / args.steps, peaks)}
         if rank == 0:
             print(json.dumps({"config": args.config, "variant": name, **results[name]}), flush=True)
         if stats is None:

@@ -19,7 +19,7 @@ from dataclasses import replace
 
 import torch
 
-from menodax_b200 import _native
+from menodax_b200 import _native, autotune
 from menodax_b200._ensemble import initial_step, launch, pick_device, solver_stats
 from menodax_b200._problem import get_problem
 
@@ -67,6 +67,17 @@ def _as_double(x, device):
     return torch.as_tensor(x, dtype=torch.float64, device=device)
 
 
+def _half_fill(problem, n: int) -> int:
+    """Blocks of the forward passes' persistent launch: half the resident limit.
+
+    Gradient ensembles are long stiff integrations with uneven step counts; the
+    refill launch keeps lanes busy as trajectories finish, and at half the
+    resident warps each runs with less contention (a 16-state ring's
+    checkpointing forward: 0.77 s against 1.21 s for the one-launch kernel;
+    unchanged for 2 states)."""
+    return autotune.grid_blocks(problem, autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5), n)
+
+
 class _EnsembleSolve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, y0, params, times, problems, dt0, rtol, atol, max_steps, key):
@@ -74,11 +85,11 @@ class _EnsembleSolve(torch.autograd.Function):
         y0c = y0.detach().contiguous()
         pc = params.detach().contiguous()
         kw = dict(y0=y0c, times=times, params=pc, weights=None, dt0=dt0, rtol=rtol, atol=atol,
-                  max_steps=max_steps, mode=_native.MDX_LAUNCH_PLAIN)
+                  max_steps=max_steps, mode=_native.MDX_LAUNCH_PERSISTENT)
         capacity, stride_hint = _capacity_hint.get(key, (None, None))
         if capacity is None:
             # First call for this problem: count the accepted steps with a plain solve.
-            _, counters = launch(problems["plain"], **kw)
+            _, counters = launch(problems["plain"], grid_blocks=_half_fill(problems["plain"], n), **kw)
             capacity = max(1, int(counters[0].max().item()) if n else 1)
         while True:
             stride = choose_stride(n, problems["plain"].n_vars, capacity, y0.device)
@@ -90,7 +101,8 @@ class _EnsembleSolve(torch.autograd.Function):
             nbytes = problem.plan.checkpoint_size(n, capacity)
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
-            hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity, **kw)
+            hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity,
+                                    grid_blocks=_half_fill(problem, n), **kw)
             needed = int(counters[0].max().item()) if n else 0
             if needed <= capacity:
                 break

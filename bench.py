@@ -391,11 +391,13 @@ def run_config(args):
             prob, mode, grid = get_problem(fn, n_vars, n_params, opts), _native.MDX_LAUNCH_PLAIN, 0
             label = "plain, 32 threads/block"
         else:
-            choice = autotune.tune(fn, n_vars, n_params, opts, tune_team=True, **common)
+            choice = autotune.tune(fn, n_vars, n_params, opts, tune_team=True,
+                                   tune_shared=opts.solver == "tsit5", **common)
             from dataclasses import replace
 
             prob = get_problem(fn, n_vars, n_params,
-                               replace(opts, threads_per_block=choice.threads_per_block, team=choice.team))
+                               replace(opts, threads_per_block=choice.threads_per_block, team=choice.team,
+                                       shared_stages=choice.shared_stages))
             mode, grid = choice.mode, autotune.grid_blocks(prob, choice, n)
             label = choice.describe()
         for _ in range(args.warmup):

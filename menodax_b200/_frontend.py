@@ -55,7 +55,7 @@ def resolve_mode(launch_mode: str) -> int:
 
 def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first_step,
         max_steps, return_stats, error_weights, launch_mode="auto", grid_blocks=0, tune_block=True,
-        tune_team=False):
+        tune_team=False, tune_shared=False):
     torch_io = _is_torch(y0, params)
     y0_t, p_t, n, n_vars = normalize_y0_params(y0, params)
     n_params = p_t.shape[1]
@@ -83,8 +83,9 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
         from menodax_b200 import autotune
 
         choice = autotune.tune(ode_fn, n_vars, n_params, options, tune_block=tune_block,
-                               tune_team=tune_team, **common)
-        options = _replace(options, threads_per_block=choice.threads_per_block, team=choice.team)
+                               tune_team=tune_team, tune_shared=tune_shared, **common)
+        options = _replace(options, threads_per_block=choice.threads_per_block, team=choice.team,
+                           shared_stages=choice.shared_stages)
         problem = get_problem(ode_fn, n_vars, n_params, options)
         mode = choice.mode
         grid_blocks = autotune.grid_blocks(problem, choice, n)

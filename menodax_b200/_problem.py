@@ -66,6 +66,9 @@ class KernelOptions:
     # Lanes per trajectory: 0 for the thread-per-trajectory kernels, else 4, 8,
     # 16 or 32 for the team kernel (Rodas5P, no sensitivities, hooks or adjoint).
     team: int = 0
+    # Tsit5: the stage vectors k1..k6 in shared memory, one column per thread
+    # (the reference's "shared" backend, modax/tsit5.py:117-139).
+    shared_stages: bool = False
 
 
 def controller_exponents(options: KernelOptions):
@@ -215,9 +218,19 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
     return "\n".join(parts) + "\n", meta
 
 
+STATIC_SHARED_MAX = 48 * 1024  # a block's static shared memory
+
+
+def tsit5_stage_bytes(n_system: int, threads_per_block: int) -> int:
+    """Shared memory of the Tsit5 kernel's stage arrays k1..k6 for one block."""
+    return 6 * n_system * threads_per_block * 8
+
+
 def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     """Generate the full NVRTC source; returns ``(source, meta)``."""
     tr = trace(ode_fn, n_vars, n_params)
+    if options.shared_stages and options.solver != "tsit5":
+        raise ValueError("shared_stages places Tsit5's stage vectors; Rodas5P's shared layout is the team kernel")
     if options.team:
         return _build_team_source(tr, n_vars, n_params, options)
     sens = _sens_layout(n_vars, n_params, options.sens)
@@ -324,6 +337,13 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     else:
         meta_tables = []
         parts.append("#define MDX_LU_SIZE 1")
+        if options.shared_stages:
+            stage_bytes = tsit5_stage_bytes(n_system, int(options.threads_per_block))
+            if stage_bytes > STATIC_SHARED_MAX:
+                raise ValueError(
+                    f"shared Tsit5 stages of {n_system} components x {options.threads_per_block} threads take "
+                    f"{stage_bytes} B of shared memory; at most {STATIC_SHARED_MAX} B")
+        parts.append(f"#define MDX_TSIT5_SHARED {1 if options.shared_stages else 0}")
         parts.append('#include "mdx_tsit5.cuh"')
         parts.append("#define MDX_SOLVER mdx::Tsit5")
     parts.append('#include "mdx_entry.cuh"')

@@ -16,7 +16,9 @@ per trajectory, its vectors and matrix in shared memory), plain and persistent.
 The thread kernel is a candidate up to ``THREAD_MAX_VARS`` states with a sparse
 LU, and for dense LUs only while the matrix stays in registers
 (``DENSE_UNROLL_MAX``): past that its matrix lives in local memory and a team is
-faster by an order of magnitude.
+faster by an order of magnitude.  For Tsit5 of up to 16 components the launches
+with the stage vectors in shared memory (the reference's "shared" backend) are
+candidates beside the register ones.
 
 Tuning is bounded in time.  The first candidate runs on the whole ensemble
 with at most ``PROBE_STEPS`` steps per trajectory.  When that finishes every
@@ -37,7 +39,13 @@ import torch
 
 from menodax_b200 import _native
 from menodax_b200._ensemble import launch
-from menodax_b200._problem import DENSE_UNROLL_MAX, get_problem, team_block_threads
+from menodax_b200._problem import (
+    DENSE_UNROLL_MAX,
+    STATIC_SHARED_MAX,
+    get_problem,
+    team_block_threads,
+    tsit5_stage_bytes,
+)
 from menodax_b200._team import TEAM_SIZES
 
 BLOCK_SIZES = (32, 64, 128)
@@ -46,6 +54,7 @@ PROBE = 4096
 PROBE_STEPS = 500
 BUDGET_S = 3.0
 TEAM_MIN_VARS = 16
+SHARED_STAGES_MAX_VARS = 16   # the reference's bound for its shared Tsit5 backend
 THREAD_MAX_VARS = 128
 
 
@@ -55,11 +64,13 @@ class LaunchChoice:
     mode: int
     grid_fill: float  # persistent: fraction of the occupancy-limited grid
     team: int = 0     # lanes per trajectory; 0 = one thread per trajectory
+    shared_stages: bool = False  # Tsit5: stage vectors in shared memory
 
     def describe(self) -> str:
         kind = "plain" if self.mode == _native.MDX_LAUNCH_PLAIN else f"persistent(fill={self.grid_fill})"
         lanes = f", team of {self.team}" if self.team else ""
-        return f"{kind}, {self.threads_per_block} threads/block{lanes}"
+        stages = ", stages in shared memory" if self.shared_stages else ""
+        return f"{kind}, {self.threads_per_block} threads/block{lanes}{stages}"
 
 
 
@@ -68,13 +79,18 @@ _cache: dict = {}
 _lock = threading.Lock()
 
 
-def candidates(block_sizes=BLOCK_SIZES, teams=()):
-    """Thread-kernel launches per block size; team launches as ``(team, threads_per_block)`` pairs."""
+def candidates(block_sizes=BLOCK_SIZES, teams=(), shared_blocks=(), shared_default=False):
+    """Thread-kernel launches per block size; team launches as ``(team, threads_per_block)``
+    pairs; Tsit5 launches with shared-memory stages per block size in ``shared_blocks``."""
     out = []
     for tpb in block_sizes:
-        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0))
+        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, 0, shared_default))
         for fill in PERSISTENT_FILL:
-            out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill))
+            out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill, 0, shared_default))
+    for tpb in shared_blocks:
+        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, 0, True))
+        for fill in PERSISTENT_FILL:
+            out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill, 0, True))
     for team, tpb in teams:
         out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, team))
         out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, 1.0, team))
@@ -111,13 +127,16 @@ def _timed_launch(problem, choice, stream, *, n, y0, times, params, weights, dt0
 
 
 def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, rtol, atol,
-         max_steps, n_save_hist=None, tune_block=True, tune_team=False):
+         max_steps, n_save_hist=None, tune_block=True, tune_team=False, tune_shared=False):
     """The fastest launch for this problem on these inputs (device tensors).
 
     With ``tune_block=False`` the block size stays ``options.threads_per_block``
     and only the launch kind and grid are chosen.  With ``tune_team`` the team
     kernel is a candidate too (for systems of ``TEAM_MIN_VARS`` states or more);
     an ``options.team`` already set is kept and only its launch kind is tuned.
+    With ``tune_shared`` (Tsit5) the launches with the stage vectors in shared
+    memory are candidates beside the register ones; ``options.shared_stages``
+    already set keeps them there.
 
     The first candidate runs once on the whole ensemble with at most
     ``PROBE_STEPS`` steps per trajectory.  If that finished every trajectory, its
@@ -143,9 +162,12 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
             blocks = ()
         else:
             blocks = BLOCK_SIZES if tune_block else (options.threads_per_block,)
-    cands = candidates(blocks, teams)
-    key = (ode_fn, n_vars, n_params, replace(options, threads_per_block=32, team=0), n, tuple(cands),
-           max_steps, torch.cuda.get_device_name(y0.device))
+    shared_blocks = ()
+    if tune_shared and options.solver == "tsit5" and not options.shared_stages and n_vars <= SHARED_STAGES_MAX_VARS:
+        shared_blocks = tuple(b for b in blocks if tsit5_stage_bytes(n_vars, b) <= STATIC_SHARED_MAX)
+    cands = candidates(blocks, teams, shared_blocks, options.shared_stages)
+    key = (ode_fn, n_vars, n_params, replace(options, threads_per_block=32, team=0, shared_stages=False), n,
+           tuple(cands), max_steps, torch.cuda.get_device_name(y0.device))
     with _lock:
         found = _cache.get(key)
     if found is not None:
@@ -153,7 +175,8 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
 
     def problem_for(choice):
         return get_problem(ode_fn, n_vars, n_params,
-                           replace(options, threads_per_block=choice.threads_per_block, team=choice.team))
+                           replace(options, threads_per_block=choice.threads_per_block, team=choice.team,
+                                   shared_stages=choice.shared_stages))
 
     buildable = []
     for choice in cands:
@@ -185,7 +208,8 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
         winner = best[1]
         fill = 1.0 if winner.team else 0.5
         persistent = [c for c in buildable if c.mode == _native.MDX_LAUNCH_PERSISTENT and c.team == winner.team
-                      and c.threads_per_block == winner.threads_per_block and c.grid_fill == fill]
+                      and c.threads_per_block == winner.threads_per_block and c.grid_fill == fill
+                      and c.shared_stages == winner.shared_stages]
         choice = persistent[0] if persistent else winner
         with _lock:
             _cache[key] = choice

@@ -5,6 +5,12 @@
 // per-trajectory vectors (y, u, k1..k7) are register arrays: every component
 // index is a compile-time constant.  State kept across steps: y, k7 (the FSAL
 // stage), t, dt, the PID error history, the save cursor and the counters.
+//
+// With MDX_TSIT5_SHARED the stages k1..k6 live in shared memory instead, the
+// reference's "shared" backend (modax/tsit5.py:117-139, 433-602): a
+// (6, n, MDX_TPB) array per block, each thread one column, so a warp's access to
+// component j of a stage is 32 consecutive doubles.  It takes 6n doubles per
+// trajectory out of the register file, which matters once n reaches ~16.
 #pragma once
 #include "mdx_common.cuh"
 
@@ -96,13 +102,36 @@ __device__ __forceinline__ bool running(const State& st, const MdxSolveArgs& a) 
   return st.save_idx < a.n_save && st.t < st.tf && st.n_steps < a.max_steps;
 }
 
+#if MDX_TSIT5_SHARED
+// One thread's column of a stage array in shared memory.  The accesses are
+// volatile so every use reads shared memory: otherwise the compiler keeps the
+// loaded stage values in registers, which is the pressure the placement is
+// there to remove (at 16 components: 236 registers and no spills, against 255
+// registers and 450 B of local-memory spills with the stages in registers).
+struct StageColumn {
+  volatile double* base;
+  __device__ __forceinline__ volatile double& operator[](int j) const { return base[j * MDX_TPB]; }
+};
+
+__device__ __forceinline__ StageColumn stage_column(int s) {
+  __shared__ double mdx_tsit5_stages[6][MDX_NS][MDX_TPB];
+  return StageColumn{&mdx_tsit5_stages[s][0][threadIdx.x]};
+}
+#endif
+
 __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   double dt_use = st.dt;
   if (dt_use > st.tf - st.t) dt_use = st.tf - st.t;
   if (dt_use < 1e-30) dt_use = 1e-30;
   const double t = st.t;
 
+#if MDX_TSIT5_SHARED
+  const StageColumn k1 = stage_column(0), k2 = stage_column(1), k3 = stage_column(2),
+                    k4 = stage_column(3), k5 = stage_column(4), k6 = stage_column(5);
+  double u[MDX_NS];
+#else
   double k1[MDX_NS], k2[MDX_NS], k3[MDX_NS], k4[MDX_NS], k5[MDX_NS], k6[MDX_NS], u[MDX_NS];
+#endif
   if (st.has_fsal) {
 #pragma unroll
     for (int j = 0; j < MDX_NS; ++j) k1[j] = st.k7[j];

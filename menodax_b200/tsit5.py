@@ -1,12 +1,17 @@
 """Tsit5 ensemble solve: the drop-in for ``modax.tsit5.solve``.
 
 Same signature and defaults as ``modax/tsit5.py:623-641``.  ``backend`` is
-accepted and validated as the reference does (``modax/tsit5.py:123-139``); the
-nine per-trajectory vectors live in registers here whatever it says, so the
-shared and local choices run the same kernel and are bit-identical.
+validated as the reference does (``modax/tsit5.py:123-139``) and picks where the
+stage vectors k1..k6 live: ``"local"`` in registers (every component index is a
+literal, so they are register arrays), ``"shared"`` in a shared-memory array of
+one column per thread, ``"auto"`` whichever the launch autotuner measures faster
+(registers when the ensemble is too small to tune).  The arithmetic is the same
+either way, so the choices give the same numbers.
 """
 
 from __future__ import annotations
+
+from dataclasses import replace
 
 from menodax_b200._frontend import run
 from menodax_b200._problem import KernelOptions
@@ -67,12 +72,14 @@ def solve(
     from menodax_b200.autograd import needs_grad, solve_with_grad
 
     if needs_grad(y0, params):
+        # The discrete adjoint's kernels keep their vectors in registers.
         return solve_with_grad(
             ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
             max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
         )
     return run(
-        ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
-        max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
-        launch_mode=launch,
+        ode_fn, y0, t_span, params, replace(options, shared_stages=backend == "shared"), rtol=rtol,
+        atol=atol, first_step=first_step, max_steps=max_steps, return_stats=return_stats,
+        error_weights=error_weights, launch_mode=launch, tune_block=backend != "shared",
+        tune_shared=backend == "auto",
     )

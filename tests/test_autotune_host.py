@@ -124,3 +124,16 @@ def test_a_fixed_team_is_only_tuned_for_its_launch_kind(fake_device, monkeypatch
     choice = _tune(fn, n, opts, rec, monkeypatch)
     assert {c.team for c, _, _ in rec.calls} == {8}
     assert (choice.team, choice.threads_per_block, choice.mode) == (8, 128, PERSISTENT)
+
+
+def test_tsit5_auto_backend_times_shared_stage_launches(fake_device, monkeypatch):
+    fn, _ = systems.make_vdp_system(8, mu=1.0, d=0.1)
+    opts = KernelOptions(solver="tsit5")
+    rec = Recorder(lambda c, m, s: 0.5 if c.shared_stages else 1.0, steps=10)
+    choice = _tune(fn, 16, opts, rec, monkeypatch, tune_shared=True)
+    assert choice.shared_stages
+    shared = {c.threads_per_block for c, _, _ in rec.calls if c.shared_stages}
+    assert shared == {32, 64}   # 128 threads of 16-component stages exceed a block's static shared memory
+    rec = Recorder(lambda c, m, s: 1.0, steps=10)
+    _tune(fn, 16, opts, rec, monkeypatch, tune_shared=False)
+    assert not any(c.shared_stages for c, _, _ in rec.calls)

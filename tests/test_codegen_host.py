@@ -179,3 +179,18 @@ def test_augmented_layout():
     state, sens = split_augmented(z.reshape(1, 1, -1), spec)
     assert state.tolist() == [[[1.0, 2.0]]]
     assert sens[0, 0].tolist() == [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]
+
+
+def test_tsit5_shared_stages_build_and_bounds():
+    """The shared-memory placement of Tsit5's stages compiles (NVRTC, no GPU),
+    is refused for Rodas5P, and is bounded by a block's static shared memory."""
+    from menodax_b200._problem import KernelOptions, STATIC_SHARED_MAX, build_source, get_problem, tsit5_stage_bytes
+
+    fn, _ = systems.make_vdp_system(8, mu=1.0, d=0.1)
+    prob = get_problem(fn, 16, 1, KernelOptions(solver="tsit5", threads_per_block=32, shared_stages=True))
+    assert "#define MDX_TSIT5_SHARED 1" in prob.source
+    assert tsit5_stage_bytes(16, 32) == 6 * 16 * 32 * 8 <= STATIC_SHARED_MAX
+    with pytest.raises(ValueError, match="shared memory"):
+        build_source(fn, 16, 1, KernelOptions(solver="tsit5", threads_per_block=128, shared_stages=True))
+    with pytest.raises(ValueError, match="team kernel"):
+        build_source(fn, 16, 1, KernelOptions(solver="rodas5P", shared_stages=True))

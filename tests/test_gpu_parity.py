@@ -181,3 +181,23 @@ def test_default_first_step_matches_explicit(solve):
     explicit = solve(fn, y0, t, p, first_step=(t[-1] - t[0]) * 1e-6, **kw)
     default = solve(fn, y0, t, p, **kw)
     assert np.array_equal(default, explicit)
+
+
+@pytest.mark.parametrize("which", ["lorenz", "vdp16"])
+def test_tsit5_shared_and_local_backends_agree(which):
+    """``backend="shared"`` moves the stage vectors to shared memory; the
+    arithmetic is unchanged, so the results are the register kernel's."""
+    if which == "lorenz":
+        cfg = systems.lorenz_config(size=512)
+        fn, y0, p, t_span = cfg["ode_fn"], cfg["y0"], cfg["params"], cfg["t_span"]
+    else:
+        fn, base = systems.make_vdp_system(8, mu=1.0, d=0.1)
+        rng = np.random.default_rng(8)
+        y0 = base[None, :] + rng.normal(0.0, 0.1, size=(512, 16))
+        p = rng.uniform(0.5, 2.0, size=(512, 1))
+        t_span = np.linspace(0.0, 10.0, 11)
+    kw = dict(rtol=1e-8, atol=1e-10, return_stats=True)
+    h_local, s_local = tsit5.solve(fn, y0, t_span, p, backend="local", **kw)
+    h_shared, s_shared = tsit5.solve(fn, y0, t_span, p, backend="shared", **kw)
+    assert np.array_equal(np.asarray(s_local["loop_steps"]), np.asarray(s_shared["loop_steps"]))
+    assert np.array_equal(h_local, h_shared)

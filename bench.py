@@ -295,6 +295,10 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
 
 
 # --------------------------------------------------------------------------- other configurations
+WARM_S = 0.5   # seconds of warm-up launches per configuration variant, at least
+WARM_MAX = 50  # and at most this many launches for it
+
+
 def config_roofline(fn, n_vars, n_params, opts, counters, n, n_save, launch_ms, peaks):
     """Algorithmic FP64 + LU-type operations of one launch (attempted steps the
     kernel reported x per-step counts of the traced problem) over its device
@@ -400,8 +404,15 @@ def run_config(args):
                                        shared_stages=choice.shared_stages))
             mode, grid = choice.mode, autotune.grid_blocks(prob, choice, n)
             label = choice.describe()
-        for _ in range(args.warmup):
+        # Warm up for the requested launches and at least WARM_S of device work:
+        # the first launches after a pause run below steady clocks (a 20 ms
+        # kernel takes 25-36 ms on its first two launches).
+        warm_start = time.perf_counter()
+        done = 0
+        while done < args.warmup or (time.perf_counter() - warm_start < WARM_S and done < WARM_MAX):
             hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
+            torch.cuda.synchronize()
+            done += 1
         barrier(world)
         ms = []
         # NVTX range per variant: ncu --nvtx --nvtx-include "timed:<variant>/" takes its launches.

@@ -329,7 +329,6 @@ def run_config(args):
     """One line per non-headline configuration: device-timed solves/s of the
     autotuned FP32-LU kernel (Tsit5: FP64) and of the plain FP64 reference-
     arithmetic kernel, plus the step statistics and the CPU oracle on a sample."""
-    import numpy as np
     import torch
 
     from menodax_b200 import _native, autotune, systems

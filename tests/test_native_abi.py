@@ -2,13 +2,12 @@
 compiles kernels with NVRTC for sm_100a, and rejects bad arguments with a
 status code instead of crashing."""
 
-import ctypes
 import re
 from pathlib import Path
 
 import pytest
 
-from menodax_b200 import _native, systems
+from menodax_b200 import systems
 from menodax_b200._problem import KernelOptions, build_source, compile_options
 
 HEADER = Path(__file__).resolve().parents[1] / "include" / "menodax.h"

@@ -215,7 +215,7 @@ def slice_bytes(n_vars: int, n_params: int, lu_size: int, lu_bytes: int, *, dens
     if not autonomous:
         doubles += n_vars
     if dense and not fast:
-        doubles += n_vars
+        doubles += 2 * n_vars
     size = 8 * doubles + lu_bytes * (8 * n_vars + lu_size)
     if dense:
         size += 4 * n_vars

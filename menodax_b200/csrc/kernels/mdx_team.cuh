@@ -60,7 +60,7 @@ struct Slice {
 #endif
   double p[MDX_NP > 0 ? MDX_NP : 1];
 #if MDX_TEAM_DENSE && !MDX_FAST
-  double fac[MDX_NV];
+  double fac[2 * MDX_NV];
 #endif
   lu_t k[8][MDX_NV];
   lu_t lu[MDX_TEAM_LU_SIZE];

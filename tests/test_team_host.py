@@ -159,8 +159,8 @@ def test_index_expressions():
 def test_slice_layout_sizes():
     # y, u, f, p (1) doubles; k[8][8] + lu[72] floats; perm[8] ints.
     assert slice_bytes(8, 1, 72, 4, dense=True, autonomous=True, fast=True) == 8 * 25 + 4 * (64 + 72) + 32
-    # Non-autonomous and reference arithmetic add dT and the multiplier column.
-    assert slice_bytes(8, 1, 72, 4, dense=True, autonomous=False, fast=False) == 8 * 41 + 4 * 136 + 32
+    # Non-autonomous and reference arithmetic add dT and two multiplier columns.
+    assert slice_bytes(8, 1, 72, 4, dense=True, autonomous=False, fast=False) == 8 * 49 + 4 * 136 + 32
     assert dense_lda(8) == 9 and dense_lda(9) == 9
 
 

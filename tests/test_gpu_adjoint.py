@@ -185,3 +185,26 @@ def test_sparse_lu_adjoint_matches_dense(lu_precision):
     np.testing.assert_allclose(hs, hd, rtol=tol, atol=1e-9)
     np.testing.assert_allclose(gys, gyd, rtol=tol, atol=tol * np.abs(gyd).max())
     np.testing.assert_allclose(gps, gpd, rtol=tol, atol=tol * np.abs(gpd).max())
+
+
+@pytest.mark.parametrize("n_osc", [1, 3])
+def test_vdp_gradient_config_matches_oracle_forward_sensitivities(oracle, n_osc):
+    """Config 5's system and loss: sum((y - target)^2) over the saves, targets
+    from mu * 1.05, y0 and mu differentiated.  The discrete adjoint of the solve
+    equals the oracle's forward sensitivities on the same step sequence (the
+    reference's sens_error_control=False), within 1e-5 relative."""
+    cfg = systems.vdp_gradient_config(n_osc, size=64)
+    t_span = np.linspace(0.0, 20.0, 6)
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    fn, y0, mu = cfg["ode_fn"], cfg["y0"], cfg["params"]
+    target = rodas5P.solve(fn, y0, t_span, mu * 1.05, **kw)
+    y = rodas5P.solve(fn, y0, t_span, mu, **kw)
+    w = 2.0 * (y - target)  # d loss / d hist
+    h, gy, gp = _grads(rodas5P.solve, fn, y0, t_span, mu, w, **kw)
+    oh, oy, op = _sens_grads(oracle, "rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), y0, t_span, mu, w,
+                             **kw)
+    np.testing.assert_allclose(h, oh, rtol=1e-9, atol=1e-12)
+    scale_y = np.abs(oy).max(axis=1, keepdims=True) + 1e-300
+    scale_p = np.abs(op).max(axis=1, keepdims=True) + 1e-300
+    assert (np.abs(gy - oy) / scale_y).max() < 1e-5
+    assert (np.abs(gp - op) / scale_p).max() < 1e-5

@@ -78,3 +78,23 @@ def test_brusselator_64_fp32_sparse_as_accurate_as_fp64(oracle):
     err32 = (np.abs(h32 - ref) / scale).max()
     err64 = (np.abs(o64 - ref) / scale).max()
     assert err32 <= 1.5 * err64 + 10 * cfg["rtol"]
+
+
+def test_vdp_ring_fp32_sparse_as_accurate_as_fp64(oracle):
+    """Config 3's product path (FP32 LU, fast arithmetic, AMD-ordered sparse LU)
+    against a tight FP64 oracle: as accurate as the FP64-LU solve at the same
+    tolerance, to 10 rtol."""
+    n_osc = 4
+    cfg = systems.vdp_ring_config(n_osc, size=128)
+    t_span = np.linspace(0.0, 30.0, 10)
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"])
+    h32 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], lu_precision="fp32",
+                        sparsity=cfg["sparsity"], **kw)
+    system = oracle.System.vdp_ring(n_osc, 1.0, 0.1)
+    ref, *_ = oracle.solve("rodas5P", system, cfg["y0"], t_span, cfg["params"], rtol=1e-12, atol=1e-14,
+                           lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, cfg["y0"], t_span, cfg["params"], lu_precision="fp64", **kw)
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    err32 = (np.abs(h32 - ref) / scale).max()
+    err64 = (np.abs(o64 - ref) / scale).max()
+    assert err32 <= 1.5 * err64 + 10 * cfg["rtol"]

@@ -220,31 +220,43 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
     with torch.no_grad():
         target = rodas5P.solve(fn, y0, t, mu * 1.05, **kw)
 
-    def value_and_grad():
+    def value_and_grad(lu_precision):
         y0_t = y0.clone().requires_grad_(True)
         p_t = mu.clone().requires_grad_(True)
-        hist, stats = rodas5P.solve(fn, y0_t, t, p_t, return_stats=True, **kw)
+        hist, stats = rodas5P.solve(fn, y0_t, t, p_t, return_stats=True, **{**kw, "lu_precision": lu_precision})
         loss = ((hist - target) ** 2).sum()
         loss.backward()
         return loss, y0_t.grad, p_t.grad, stats
 
-    for _ in range(warmup):
-        value_and_grad()
-    barrier(world)
     stream = torch.cuda.current_stream(dev)
-    ms = []
-    for _ in range(steps):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        loss, gy, gp, stats = value_and_grad()
-        e1.record(stream)
-        ms.append((e0, e1))
-    barrier(world)
-    per = [a.elapsed_time(b) for a, b in ms]
-    total = max_over_ranks(sum(per), world)
+
+    def timed(lu_precision, n_steps):
+        for _ in range(warmup):
+            value_and_grad(lu_precision)
+        barrier(world)
+        ms = []
+        for _ in range(n_steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            loss, gy, gp, stats = value_and_grad(lu_precision)
+            e1.record(stream)
+            ms.append((e0, e1))
+        barrier(world)
+        total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
+        return total, gy, gp, stats
+
+    total, gy, gp, stats = timed("fp64", steps)
     acc = stats["accepted_steps"].to(torch.float64)
     finite = bool(torch.isfinite(gy).all() and torch.isfinite(gp).all())
+    # The FP32-LU adjoint (fast arithmetic) on the same ensemble: its own step
+    # sequence, so its gradients differ from the FP64 ones at solver-tolerance
+    # level; the median relative difference says by how much.
+    fs32 = max(1, steps // 2)
+    total32, gy32, gp32, _ = timed("fp32", fs32)
+    g64 = torch.cat([gy, gp], dim=1)
+    g32 = torch.cat([gy32, gp32], dim=1)
+    rel32 = (g32 - g64).abs().max(dim=1).values / g64.abs().max(dim=1).values.clamp_min(1e-300)
 
     result = {
         "metric": "gradients/s", "value": n * world * steps / (total * 1e-3), "unit": "gradients/s",
@@ -254,6 +266,12 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
                     f"{n} trajectories per GPU, 20 saves on [0, 1000], rtol 1e-6, atol 1e-8",
         "accepted_steps_mean": float(acc.mean()), "accepted_steps_max": float(acc.max()),
         "gradients_finite": finite,
+        "fp32_lu": {
+            "value": n * world * fs32 / (total32 * 1e-3), "unit": "gradients/s",
+            "ms_per_step": total32 / fs32,
+            "method": "the same discrete adjoint with FP32 LUs and fast arithmetic",
+            "median_rel_diff_vs_fp64": float(rel32.median()),
+        },
     }
     if n_osc > 1:
         # The joint [y, S] system of forward sensitivities would carry

@@ -19,10 +19,11 @@ def benchmark_problems():
     for tpb in (32, 64, 128):
         out.append((systems.robertson, 3, 3, KernelOptions(lu_precision="fp32", fast=True, threads_per_block=tpb)))
     vdp = systems.vdp_gradient_config(1, size=1)["ode_fn"]
-    out.append((vdp, 2, 1, KernelOptions(lu_precision="fp64")))
-    for stride in (1, 8, 32):
-        out.append((vdp, 2, 1, KernelOptions(lu_precision="fp64", checkpoint=True, adjoint=True,
-                                              ckpt_stride=stride)))
+    for prec, fast in (("fp64", False), ("fp32", True)):
+        out.append((vdp, 2, 1, KernelOptions(lu_precision=prec, fast=fast)))
+        for stride in (1, 8, 32):
+            out.append((vdp, 2, 1, KernelOptions(lu_precision=prec, fast=fast, checkpoint=True, adjoint=True,
+                                                  ckpt_stride=stride)))
     return out
 
 

@@ -238,6 +238,9 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
         for _ in range(n_steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            # Each step starts on an idle device, so no step's time holds the
+            # tail of the one before.
+            torch.cuda.synchronize(dev)
             e0.record(stream)
             loss, gy, gp, stats = value_and_grad(lu_precision)
             e1.record(stream)

@@ -264,8 +264,8 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
     _, updates, substitutions = layout.flop_counts()
     out = []
     # The reciprocal pivot: double then rounded, as the reference types it; in the
-    # fast path a division in the LU type.
-    recip = "(T)1 / lu[{0}]" if fast else "(T)(1.0 / (double)lu[{0}])"
+    # fast path mdx::fast_recip in the LU type (approximate in FP32).
+    recip = "mdx::fast_recip(lu[{0}])" if fast else "(T)(1.0 / (double)lu[{0}])"
 
     unroll_factor = mode == "unrolled" or (mode == "auto" and destination.size <= MAX_UNROLLED_UPDATES)
     unroll_solve = mode == "unrolled" or (mode == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS)

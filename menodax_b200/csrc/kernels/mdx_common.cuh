@@ -34,16 +34,32 @@ __device__ __forceinline__ double fast_pow(double x, double e) {
   return (double)__powf((float)x, (float)e);
 }
 
+// 1/x for the fast path's LU pivots.  In single precision the approximate
+// reciprocal (__fdividef: within 2 ulp for |x| in [2^-126, 2^126], 1/0 = inf),
+// whose error is below the FP32 factorisation's own rounding; double pivots keep
+// the IEEE division.
+__device__ __forceinline__ float fast_recip(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double fast_recip(double x) { return 1.0 / x; }
+
+// 1/s in double for the fast path (the step's 1/h, the error scales): the
+// single-precision reciprocal as a seed, refined by one Newton-Raphson step
+// y <- y + y (1 - s y), which squares the seed's relative error (~1e-7 ->
+// ~1e-14).  Values outside float's normal range keep the IEEE division.
+__device__ __forceinline__ double recip_newton(double s) {
+  if (s >= 1e-37 && s <= 1e37) {
+    const double y = (double)__fdividef(1.0f, (float)s);
+    return fma(y, fma(-s, y, 1.0), y);
+  }
+  return 1.0 / s;
+}
+
 // Step-size controller (modax/rodas5P.py:913-928, modax/tsit5.py:383-398):
 // clamp the error into [1e-18, 1e18] (NaN counts as huge), form the PID factor
 // from the error history, and clamp the factor.  E2 and E3 are compile-time
-// constants, so the default I-controller multiplies by nothing extra.  FAST
-// evaluates the powers in float.
-template <bool FAST>
-__device__ __forceinline__ double controller_factor(double err_norm, double err_prev,
-                                                    double err_prev2, double e1, double e2,
-                                                    double e3, bool use_e2, bool use_e3,
-                                                    double& safe_err) {
+// constants, so the default I-controller multiplies by nothing extra.
+__device__ __forceinline__ double controller_factor(double err_norm, double err_prev, double err_prev2,
+                                                    double e1, double e2, double e3, bool use_e2,
+                                                    bool use_e3, double& safe_err) {
   if (isnan(err_norm) || err_norm > 1e18) {
     safe_err = 1e18;
   } else if (err_norm == 0.0) {
@@ -51,15 +67,30 @@ __device__ __forceinline__ double controller_factor(double err_norm, double err_
   } else {
     safe_err = err_norm;
   }
-  if (FAST) {
-    double factor = 0.9 * fast_pow(safe_err, e1);
-    if (use_e2) factor = factor * fast_pow(err_prev, e2);
-    if (use_e3) factor = factor * fast_pow(err_prev2, e3);
-    return factor;
-  }
   double factor = 0.9 * pow(safe_err, e1);
   if (use_e2) factor = factor * pow(err_prev, e2);
   if (use_e3) factor = factor * pow(err_prev2, e3);
+  return factor;
+}
+
+// The fast path's controller on the SQUARED weighted RMS error: the step is
+// accepted on err^2 <= 1 and err^e = (err^2)^(e/2), so no square root is taken.
+// The error history is kept squared too.  The clamp is [1e-36, 1e36] on err^2
+// (the reference's [1e-18, 1e18] on err), applied below as well as at zero so
+// that every power is taken of a normal float.
+__device__ __forceinline__ double controller_factor_sq(double err_sq, double prev_sq, double prev2_sq,
+                                                       double e1, double e2, double e3, bool use_e2,
+                                                       bool use_e3, double& safe_sq) {
+  if (isnan(err_sq) || err_sq > 1e36) {
+    safe_sq = 1e36;
+  } else if (err_sq < 1e-36) {
+    safe_sq = 1e-36;
+  } else {
+    safe_sq = err_sq;
+  }
+  double factor = 0.9 * fast_pow(safe_sq, 0.5 * e1);
+  if (use_e2) factor = factor * fast_pow(prev_sq, 0.5 * e2);
+  if (use_e3) factor = factor * fast_pow(prev2_sq, 0.5 * e3);
   return factor;
 }
 

@@ -168,8 +168,8 @@ __device__ __forceinline__ void dense_solve_t(const LU& lu, const IP& ipiv, R& r
 // The factorisation runs entirely in T (no double multipliers, no conversions),
 // the row swaps are folded into a permutation `perm` (perm[i] = the original
 // row that ends at position i) so a solve permutes its right-hand side with
-// selects instead of branches, and the diagonal is left holding 1/U_ii so the
-// back substitution multiplies.  Same algorithm, different rounding: the FP32
+// selects instead of branches, and the diagonal is left holding 1/U_ii (the
+// approximate reciprocal fast_recip) so the back substitution multiplies.  Same algorithm, different rounding: the FP32
 // path is held to accuracy against the FP64 oracle, not to the reference's bits.
 template <int N, typename T, class LU, class IP>
 __device__ __forceinline__ void dense_factorize_fast(LU& lu, IP& perm) {
@@ -199,7 +199,8 @@ __device__ __forceinline__ void dense_factorize_fast(LU& lu, IP& perm) {
       perm[k] = sw ? pa : pb;
     }
     const T piv = lu[i * N + i];
-    const T inv_piv = piv != T(0) ? T(1) / piv : T(0);
+    const T recip = fast_recip(piv);
+    const T inv_piv = piv != T(0) ? recip : T(0);
 #pragma unroll
     for (int k = i + 1; k < N; ++k) {
       const T factor = lu[k * N + i] * inv_piv;
@@ -207,7 +208,7 @@ __device__ __forceinline__ void dense_factorize_fast(LU& lu, IP& perm) {
 #pragma unroll
       for (int j = i + 1; j < N; ++j) lu[k * N + j] -= factor * lu[i * N + j];
     }
-    lu[i * N + i] = T(1) / piv;
+    lu[i * N + i] = recip;
   }
 }
 

@@ -235,12 +235,13 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
   double dt_use = st.dt;
   if (dt_use > st.tf_local - st.t) dt_use = st.tf_local - st.t;
   if (dt_use < 1e-30) dt_use = 1e-30;
-  const double inv_dt = 1.0 / dt_use;
   const double t = st.t;
   const double t_end = t + dt_use;
 #if MDX_FAST
+  const double inv_dt = recip_newton(dt_use);
   const double dtgamma_inv = inv_dt * (1.0 / GAMMA);
 #else
+  const double inv_dt = 1.0 / dt_use;
   const double dtgamma_inv = 1.0 / (dt_use * GAMMA);
 #endif
 
@@ -286,22 +287,29 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
     const double k7 = (double)s.k[7][j];
     const double y_new_j = s.u[j] + k7;
     const double scale = a.atol + a.rtol * pymax(fabs(s.y[j]), fabs(y_new_j));
+#if MDX_FAST
+    s.f[j] = weight(a, st.traj, j) * k7 * recip_newton(scale);
+#else
     s.f[j] = weight(a, st.traj, j) * k7 / scale;
+#endif
   }
   __syncwarp(L.mask);
   double err_local = 0.0;
 #pragma unroll 8
   for (int j = 0; j < MDX_NV; ++j) err_local += s.f[j] * s.f[j];
+  double safe_err;
 #if MDX_FAST
-  const double err_norm = sqrt(err_local * (1.0 / MDX_NERR));
+  // Squared norm and history (controller_factor_sq): no square root.
+  const double err_sq = err_local * (1.0 / MDX_NERR);
+  const bool accept = err_sq <= 1.0;
+  double factor = controller_factor_sq(err_sq, st.err_prev, st.err_prev2, MDX_E1, MDX_E2, MDX_E3,
+                                       MDX_USE_E2, MDX_USE_E3, safe_err);
 #else
   const double err_norm = sqrt(err_local / MDX_NERR);
-#endif
   const bool accept = err_norm <= 1.0 && !isnan(err_norm);
-
-  double safe_err;
-  double factor = controller_factor<MDX_FAST>(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2,
-                                              MDX_E3, MDX_USE_E2, MDX_USE_E3, safe_err);
+  double factor = controller_factor(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2, MDX_E3,
+                                    MDX_USE_E2, MDX_USE_E3, safe_err);
+#endif
   if (accept) {
     st.err_prev2 = st.err_prev;
     st.err_prev = safe_err;

@@ -27,12 +27,13 @@ __device__ __forceinline__ T not_nan_or(T v, T fallback) { return v == v ? v : f
 // butterfly that prefers the larger magnitude and, on a tie, the smaller row --
 // the serial scan's first maximum.  A NaN never wins (the serial scan keeps the
 // diagonal then; the step's error estimate is NaN either way and rejects).  The
-// pivot row is swapped into place over every column, with the permutation and,
-// when given, a pending multiplier column `fac0` that belongs to the rows.
+// pivot row is swapped into place over every column, with the permutation and
+// the `pending` multiplier columns fac[m * N + row] (m < pending) that belong to
+// the rows.
 template <int N, int LDA, typename T>
 __device__ __forceinline__ void pivot_swap(T* __restrict__ a, int* __restrict__ perm,
-                                           double* __restrict__ fac0, const int c, const int lane,
-                                           const unsigned mask) {
+                                           double* __restrict__ fac, const int pending, const int c,
+                                           const int lane, const unsigned mask) {
   T best = T(-1);
   int bi = N;
   for (int r = c + lane; r < N; r += MDX_TEAM) {
@@ -56,10 +57,10 @@ __device__ __forceinline__ void pivot_swap(T* __restrict__ a, int* __restrict__ 
       const int p = perm[c];
       perm[c] = perm[bi];
       perm[bi] = p;
-      if (fac0) {
-        const double f = fac0[c];
-        fac0[c] = fac0[bi];
-        fac0[bi] = f;
+      for (int m = 0; m < pending; ++m) {
+        const double f = fac[m * N + c];
+        fac[m * N + c] = fac[m * N + bi];
+        fac[m * N + bi] = f;
       }
     }
   }
@@ -67,7 +68,7 @@ __device__ __forceinline__ void pivot_swap(T* __restrict__ a, int* __restrict__ 
 }
 
 // Multipliers of column c below the diagonal.  FAST: in T, stored in place, the
-// diagonal replaced by its reciprocal.  Otherwise the reference's typing:
+// diagonal replaced by its reciprocal (fast_recip).  Otherwise the reference's typing:
 // double multipliers kept unrounded in `fac` for the updates, rounded into the
 // matrix, nothing done for a zero pivot.  Returns whether updates from column c
 // apply.
@@ -76,10 +77,11 @@ __device__ __forceinline__ bool multipliers(T* __restrict__ a, double* __restric
                                             const int lane, const unsigned mask) {
   const T piv = a[c * LDA + c];
   if constexpr (FAST) {
-    const T inv = piv != T(0) ? T(1) / piv : T(0);
+    const T recip = fast_recip(piv);
+    const T inv = piv != T(0) ? recip : T(0);
     for (int r = c + 1 + lane; r < N; r += MDX_TEAM) a[r * LDA + c] *= inv;
     __syncwarp(mask);
-    if (lane == 0) a[c * LDA + c] = T(1) / piv;
+    if (lane == 0) a[c * LDA + c] = recip;
     return true;
   } else {
     if (piv == T(0)) return false;
@@ -104,69 +106,102 @@ __device__ __forceinline__ T eliminate(T x, T l, double f, T u) {
   }
 }
 
-// Columns are eliminated two at a time.  Column c is pivoted and scaled; its
-// update is applied at once only to column c + 1 (which the next pivot search
-// reads); column c + 1 is pivoted and scaled; row c + 1 takes column c's update;
-// then one pass over the trailing rows applies both updates, entry by entry in
+// Columns are eliminated in panels of W.  Within a panel, column c + k first
+// takes the updates of the panel's earlier columns (its rows c+1 .. c+k-1 in
+// order on one lane, then its rows from c + k down on all lanes), is pivoted and
+// scaled, and row c + k right of the panel takes the earlier columns' updates.
+// One pass over the trailing rows then applies the W updates, entry by entry in
 // the order the one-column algorithm applies them, so every entry rounds the same
-// way.  A row swap between the two steps moves un-updated trailing entries
-// together with the multipliers that update them.  The pass reads each trailing
-// entry once and writes it once for two FMAs, with the two multipliers of its row
-// read once for all of a lane's columns and the lane's two pivot-row entries held
-// in registers -- half the shared-memory traffic per FMA of a one-column pass.
+// way as there.  A row swap inside a panel moves un-updated entries together with
+// the multipliers that update them.  The pass reads each trailing entry once and
+// writes it once for W FMAs, the W multipliers of its row read once for all of a
+// lane's columns and the lane's W pivot-row entries held in registers.
+//
+// FAST keeps no double multipliers and takes W = 4 (W = 2 when a lane's pivot-row
+// entries would take too many registers); the reference's arithmetic takes W = 2
+// with the two double multiplier columns in `fac`.
 template <int N, int LDA, typename T, bool FAST>
 __device__ __forceinline__ void dense_factorize(T* __restrict__ a, int* __restrict__ perm,
                                                 double* __restrict__ fac, const int lane,
                                                 const unsigned mask) {
   constexpr int NB = (N + MDX_TEAM - 1) / MDX_TEAM;
-  double* fac0 = FAST ? nullptr : fac;
-  double* fac1 = FAST ? nullptr : fac + N;
+  constexpr int W = (FAST && NB <= 4) ? 4 : 2;
   for (int i = lane; i < N; i += MDX_TEAM) perm[i] = i;
   __syncwarp(mask);
 #pragma unroll 1
-  for (int c = 0; c < N; c += 2) {
-    pivot_swap<N, LDA, T>(a, perm, nullptr, c, lane, mask);
-    const bool on0 = multipliers<N, LDA, T, FAST>(a, fac0, c, lane, mask);
-    if (c + 1 >= N) break;
-    const int c1 = c + 1;
-    // Column c + 1 below row c takes column c's update.
-    if (on0) {
-      const T u = a[c * LDA + c1];
-      for (int r = c1 + lane; r < N; r += MDX_TEAM)
-        a[r * LDA + c1] = eliminate<T, FAST>(a[r * LDA + c1], a[r * LDA + c], FAST ? 0.0 : fac0[r], u);
-    }
-    __syncwarp(mask);
-    pivot_swap<N, LDA, T>(a, perm, fac0, c1, lane, mask);
-    const bool on1 = multipliers<N, LDA, T, FAST>(a, fac1, c1, lane, mask);
-    // Row c + 1 right of the pair takes column c's update.
-    if (on0) {
-      const T l = a[c1 * LDA + c];
-      const double f = FAST ? 0.0 : fac0[c1];
-      for (int j = c1 + 1 + lane; j < N; j += MDX_TEAM)
-        a[c1 * LDA + j] = eliminate<T, FAST>(a[c1 * LDA + j], l, f, a[c * LDA + j]);
-    }
-    __syncwarp(mask);
-    // Rows below the pair, columns right of it: both updates in one pass.
-    T u0[NB], u1[NB];
+  for (int c = 0; c < N; c += W) {
+    const int w = N - c < W ? N - c : W;
+    bool on[W];
 #pragma unroll
-    for (int q = 0; q < NB; ++q) {
-      const int j = c1 + 1 + lane + q * MDX_TEAM;
-      u0[q] = j < N ? a[c * LDA + j] : T(0);
-      u1[q] = j < N ? a[c1 * LDA + j] : T(0);
+    for (int k = 0; k < W; ++k) {
+      on[k] = false;
+      if (k >= w) continue;
+      const int ck = c + k;
+      if (k > 0) {
+        // Column ck, rows c+1 .. ck-1 (finished rows of U): serial in the row.
+        if (lane == 0) {
+#pragma unroll
+          for (int ii = 1; ii < k; ++ii) {
+            const int i = c + ii;
+            T x = a[i * LDA + ck];
+#pragma unroll
+            for (int m = 0; m < ii; ++m)
+              if (on[m]) x = eliminate<T, FAST>(x, a[i * LDA + c + m], FAST ? 0.0 : fac[m * N + i], a[(c + m) * LDA + ck]);
+            a[i * LDA + ck] = x;
+          }
+        }
+        __syncwarp(mask);
+        // Column ck from row ck down: the pivot search reads these.
+        for (int r = ck + lane; r < N; r += MDX_TEAM) {
+          T x = a[r * LDA + ck];
+#pragma unroll
+          for (int m = 0; m < k; ++m)
+            if (on[m]) x = eliminate<T, FAST>(x, a[r * LDA + c + m], FAST ? 0.0 : fac[m * N + r], a[(c + m) * LDA + ck]);
+          a[r * LDA + ck] = x;
+        }
+        __syncwarp(mask);
+      }
+      pivot_swap<N, LDA, T>(a, perm, fac, FAST ? 0 : k, ck, lane, mask);
+      on[k] = multipliers<N, LDA, T, FAST>(a, FAST ? nullptr : fac + k * N, ck, lane, mask);
+      if (k > 0) {
+        // Row ck right of the panel.
+        for (int j = c + w + lane; j < N; j += MDX_TEAM) {
+          T x = a[ck * LDA + j];
+#pragma unroll
+          for (int m = 0; m < k; ++m)
+            if (on[m]) x = eliminate<T, FAST>(x, a[ck * LDA + c + m], FAST ? 0.0 : fac[m * N + ck], a[(c + m) * LDA + j]);
+          a[ck * LDA + j] = x;
+        }
+        __syncwarp(mask);
+      }
     }
-#pragma unroll 2
-    for (int r = c1 + 1; r < N; ++r) {
-      const T l0 = a[r * LDA + c];
-      const T l1 = a[r * LDA + c1];
-      const double f0 = FAST ? 0.0 : fac0[r];
-      const double f1 = FAST ? 0.0 : fac1[r];
+    // Rows below the panel, columns right of it: the W updates in one pass.
+    T u[W][NB];
+#pragma unroll
+    for (int m = 0; m < W; ++m) {
 #pragma unroll
       for (int q = 0; q < NB; ++q) {
-        const int j = c1 + 1 + lane + q * MDX_TEAM;
+        const int j = c + w + lane + q * MDX_TEAM;
+        u[m][q] = (m < w && j < N) ? a[(c + m) * LDA + j] : T(0);
+      }
+    }
+#pragma unroll 2
+    for (int r = c + w; r < N; ++r) {
+      T l[W];
+      double f[W];
+#pragma unroll
+      for (int m = 0; m < W; ++m) {
+        l[m] = m < w ? a[r * LDA + c + m] : T(0);
+        f[m] = (FAST || m >= w) ? 0.0 : fac[m * N + r];
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+        const int j = c + w + lane + q * MDX_TEAM;
         if (j < N) {
           T x = a[r * LDA + j];
-          if (on0) x = eliminate<T, FAST>(x, l0, f0, u0[q]);
-          if (on1) x = eliminate<T, FAST>(x, l1, f1, u1[q]);
+#pragma unroll
+          for (int m = 0; m < W; ++m)
+            if (on[m]) x = eliminate<T, FAST>(x, l[m], f[m], u[m][q]);
           a[r * LDA + j] = x;
         }
       }

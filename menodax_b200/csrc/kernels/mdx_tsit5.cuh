@@ -209,8 +209,8 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   }
 
   double safe_err;
-  double factor = controller_factor<false>(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2,
-                                           MDX_E3, MDX_USE_E2, MDX_USE_E3, safe_err);
+  double factor = controller_factor(err_norm, st.err_prev, st.err_prev2, MDX_E1, MDX_E2, MDX_E3,
+                                    MDX_USE_E2, MDX_USE_E3, safe_err);
   if (accept) {
     st.err_prev2 = st.err_prev;
     st.err_prev = safe_err;

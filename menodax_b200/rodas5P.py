@@ -78,9 +78,12 @@ def solve(
     controller are always double.  ``arithmetic="reference"`` rounds exactly
     where the reference does (double multipliers in the LU, divisions in the
     substitutions, a double-precision controller power); ``"fast"`` runs the LU
-    wholly in the LU type with the reciprocal diagonal multiplied in and the
-    controller power in float.  ``"auto"`` is fast for ``lu_precision="fp32"``
-    and reference for ``"fp64"``.  ``sparsity`` (a mask, a scipy sparse matrix or
+    wholly in the LU type with the reciprocal diagonal multiplied in (in FP32
+    the approximate reciprocal), forms 1/h and the error scales' reciprocals
+    from a float seed and one double Newton step, and takes the controller
+    power of the squared error norm in float (no square root).  ``"auto"`` is
+    fast for ``lu_precision="fp32"`` and reference for ``"fp64"``.
+    ``sparsity`` (a mask, a scipy sparse matrix or
     ``(nnz, 2)`` pairs) colours the Jacobian sweep and compiles a sparse LU for the
     pattern, ordered by ``ordering`` (``"amd"`` or ``"natural"``).  ``tf_index``
     names a parameter column holding each trajectory's own end time.

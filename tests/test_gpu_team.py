@@ -40,7 +40,7 @@ def test_team_vdp_ring_fp64_matches_oracle(oracle, team, layout):
     np.testing.assert_allclose(hist[same], h[same], rtol=1e-9, atol=1e-12)
 
 
-@pytest.mark.parametrize("team", [8, 32])
+@pytest.mark.parametrize("team", [8, 16, 32])
 @pytest.mark.parametrize("layout", ["sparse", "dense"])
 def test_team_brusselator_64_fp32_as_accurate_as_fp64(oracle, team, layout):
     cfg = systems.brusselator_config(n_grid=32, size=128)
@@ -56,6 +56,46 @@ def test_team_brusselator_64_fp32_as_accurate_as_fp64(oracle, team, layout):
     err32 = (np.abs(h32 - ref) / scale).max()
     err64 = (np.abs(o64 - ref) / scale).max()
     assert err32 <= 1.5 * err64 + 10 * cfg["rtol"]
+
+
+@pytest.mark.parametrize("n_grid,team", [(15, 8), (12, 16)])
+def test_team_dense_fp32_panels_as_accurate_as_fp64(oracle, n_grid, team):
+    """The fast dense LU's four-column panels (each lane's pivot-row entries in
+    registers): 30 states on 8 lanes end on a two-column panel, 24 on 16 lanes
+    divide evenly."""
+    cfg = systems.brusselator_config(n_grid=n_grid, size=128)
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"])
+    h32 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], lu_precision="fp32",
+                        team=team, launch="plain", **kw)
+    system = oracle.System.brusselator(n_grid)
+    ref, *_ = oracle.solve("rodas5P", system, cfg["y0"], cfg["t_span"], cfg["params"], rtol=1e-12,
+                           atol=1e-14, lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, cfg["y0"], cfg["t_span"], cfg["params"], lu_precision="fp64",
+                           **kw)
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    err32 = (np.abs(h32 - ref) / scale).max()
+    err64 = (np.abs(o64 - ref) / scale).max()
+    assert err32 <= 1.5 * err64 + 10 * cfg["rtol"]
+
+
+@pytest.mark.parametrize("n_osc", [5, 6])
+def test_team_dense_panels_factor_like_the_thread_kernel(n_osc):
+    """Fast arithmetic in FP64: the thread kernel's register LU and the team's
+    four-column panels (4 lanes: 10 states end on a two-column panel, 12 divide
+    evenly) apply the same operations to every entry in the same order, so the
+    factorisations agree bit for bit and only the substitutions' summation order
+    differs (measured: at most 1.6e-10 apart on O(1) states, a handful of entries
+    in 1e5 above 1e-9 relative).  A missed or misordered update would put the two
+    runs rtol apart."""
+    cfg = systems.vdp_ring_config(n_osc, size=512)
+    t_span = np.linspace(0.0, 30.0, 20)
+    kw = dict(rtol=1e-6, atol=1e-8, lu_precision="fp64", arithmetic="fast", launch="plain",
+              return_stats=True)
+    h0, s0 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], team=0, **kw)
+    h4, s4 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], team=4, **kw)
+    same = np.asarray(s0["loop_steps"]) == np.asarray(s4["loop_steps"])
+    assert same.mean() >= 0.999
+    np.testing.assert_allclose(h4[same], h0[same], rtol=1e-9, atol=1e-9)
 
 
 @pytest.mark.parametrize("team", [4, 16])

@@ -53,15 +53,16 @@ namespace adjoint {
 using namespace mdx::rodas5p;
 
 // Recompute one accepted Rodas5P step from its start state exactly as the
-// forward step did: the factorised iteration matrix, the eight stages and the
-// point each stage's f was evaluated at.  The end state is us[7] + k[7].
+// forward step did (the same 1/h and 1/(h gamma), step_reciprocals): the
+// factorised iteration matrix, the eight stages and the point each stage's f was
+// evaluated at.  The end state is us[7] + k[7].
 template <class LU, class IP, class K, class US, class DTV>
 __device__ __forceinline__ void recompute(double t, double h, const double (&y)[MDX_NV], const double* p,
                                           LU& lu, IP& ipiv, K& k, US& us, DTV& dT) {
   typedef MDX_LU_T T;
-  const double inv_dt = 1.0 / h;
+  double inv_dt, dtgamma_inv;
+  step_reciprocals(h, inv_dt, dtgamma_inv);
   const double t_end = t + h;
-  const double dtgamma_inv = 1.0 / (h * GAMMA);
   mdx_neg_jac(y, t, p, lu, dT);
 #pragma unroll
   for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (T)dtgamma_inv;
@@ -131,7 +132,8 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
                                              int s_lo, int s_hi, double (&ybar)[MDX_NV],
                                              double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
   typedef MDX_LU_T T;
-  const double inv_dt = 1.0 / h;
+  double inv_dt, dtgamma_inv;
+  step_reciprocals(h, inv_dt, dtgamma_inv);
   const double t_end = t + h;
   T lu[MDX_LU_SIZE];
   int ipiv[MDX_IPIV];

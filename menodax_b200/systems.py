@@ -214,6 +214,30 @@ def forced_decay(y, t, p):
     return (-p[0] * y[0] + p[1] * t,)
 
 
+def decay_chain(y, t, p):
+    """A -> B -> C -> D with rates p[0], p[1], p[2] (the reference's
+    tests/test_sparsity.py:40-46); D is stable, so the total is conserved."""
+    return (
+        -p[0] * y[0],
+        p[0] * y[0] - p[1] * y[1],
+        p[1] * y[1] - p[2] * y[2],
+        p[2] * y[2],
+    )
+
+
+DECAY_CHAIN_PATTERN = [(0, 0), (1, 0), (1, 1), (2, 1), (2, 2), (3, 2)]
+
+
+def decay_chain_exact(t: float, a: float, b: float, c: float) -> np.ndarray:
+    """The chain's state at t from (1, 0, 0, 0), distinct rates a, b, c:
+    the Bateman sums over exp(-rate t) for B and C, D from conservation."""
+    ea, eb, ec = math.exp(-a * t), math.exp(-b * t), math.exp(-c * t)
+    y0 = ea
+    y1 = a / (b - a) * (ea - eb)
+    y2 = a * b * (ea / ((b - a) * (c - a)) + eb / ((a - b) * (c - b)) + ec / ((a - c) * (b - c)))
+    return np.array([y0, y1, y2, 1.0 - y0 - y1 - y2])
+
+
 def rate_scale_params(size: int, seed: int = 42) -> np.ndarray:
     """p[0] = 1 + 0.1 * U[-1, 1) per trajectory: the rate scale of the linear
     closed-form systems below (reference/systems/python/{kaps,bateman,heat}.py)."""

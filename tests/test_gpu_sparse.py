@@ -105,3 +105,36 @@ def test_vdp_ring_fp32_sparse_as_accurate_as_fp64(oracle):
     for q in (0.5, 0.9):
         assert np.quantile(err32, q) <= 1.5 * np.quantile(err64, q) + 10 * cfg["rtol"]
     assert err32.max() <= 3.0 * err64.max()
+
+
+def test_decay_chain_sparse_solves_what_dense_solves():
+    """tests/test_sparsity.py:110-127: a pattern changes the sweeps and the
+    factorisation, not the answer; the chain's state at t = 2 is its closed form."""
+    y0 = np.tile(np.array([1.0, 0.0, 0.0, 0.0]), (64, 1))
+    p = np.tile(np.array([0.7, 0.4, 0.2]), (64, 1))
+    t = np.array([0.0, 0.5, 2.0])
+    kw = dict(rtol=1e-11, atol=1e-13, first_step=1e-4, lu_precision="fp64")
+    dense = rodas5P.solve(systems.decay_chain, y0, t, p, **kw)
+    sparse = rodas5P.solve(systems.decay_chain, y0, t, p, sparsity=systems.DECAY_CHAIN_PATTERN, **kw)
+    np.testing.assert_allclose(sparse, dense, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(sparse[0, -1], systems.decay_chain_exact(2.0, 0.7, 0.4, 0.2), rtol=1e-9,
+                               atol=1e-11)
+
+
+def test_decay_chain_gradients_survive_the_sparse_lu():
+    """tests/test_sparsity.py:130-144: the gradient of sum(y(2)^2) in the rates is
+    the same with and without the pattern (here by the discrete adjoint)."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    y0 = torch.tensor([[1.0, 0.0, 0.0, 0.0]], dtype=torch.float64, device=dev)
+    t = np.array([0.0, 2.0])
+    kw = dict(rtol=1e-11, atol=1e-13, first_step=1e-4, lu_precision="fp64")
+
+    def grad(**extra):
+        p = torch.tensor([[0.7, 0.4, 0.2]], dtype=torch.float64, device=dev, requires_grad=True)
+        out = rodas5P.solve(systems.decay_chain, y0, t, p, **kw, **extra)
+        (out[0, -1] ** 2).sum().backward()
+        return p.grad.cpu().numpy()
+
+    np.testing.assert_allclose(grad(sparsity=systems.DECAY_CHAIN_PATTERN), grad(), rtol=1e-9)

@@ -208,6 +208,14 @@ def test_tridiagonal_takes_three_colours():
     assert colour_sparsity(normalize_sparsity(mask, n)).n_colours == 3
 
 
+def test_decay_chain_takes_two_colours():
+    """tests/test_sparsity.py:114-116: the chain's four columns in two sweeps."""
+    from menodax_b200 import systems
+
+    compressed = colour_sparsity(normalize_sparsity(systems.DECAY_CHAIN_PATTERN, 4))
+    assert compressed.n_colours == 2
+
+
 def test_dense_is_row_major():
     d = dense_jacobian(4)
     assert [d.slot(r, c) for r in range(4) for c in range(4)] == list(range(16))

@@ -316,9 +316,11 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
             fwd.append(f"  rhs[{row}] = rhs[{row}]{terms};")
         for i in range(n - 1, -1, -1):
             row, pivot = int(origin[i]), int(diag_ptr[i])
-            terms = "".join(
-                f" - lu[{p}] * rhs[{int(col_origin[p])}]" for p in range(pivot + 1, int(row_ptr[i + 1]))
-            )
+            upper = range(pivot + 1, int(row_ptr[i + 1]))
+            # The fast path subtracts the back substitution's terms latest-solved
+            # last (descending column), so a row waits on one FMA after its last
+            # input instead of on all of them; the reference's order is ascending.
+            terms = "".join(f" - lu[{p}] * rhs[{int(col_origin[p])}]" for p in (reversed(upper) if fast else upper))
             back.append(f"  rhs[{row}] = (rhs[{row}]{terms}) * lu[{pivot}];")
         # Transposed: U^T z = b by rows of U in elimination order (scatter),
         # then L^T w = z by rows of L in reverse order (scatter).
@@ -352,8 +354,10 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
             "    rhs[row] = acc;\n  }\n"
             f"  for (int i = {n - 1}; i >= 0; --i) {{\n"
             "    const int row = mdx_sv_origin[i]; const int pivot = mdx_sv_diag[i]; T acc = rhs[row];\n"
-            "    for (int p = pivot + 1; p < mdx_sv_row[i + 1]; ++p) acc -= lu[p] * rhs[mdx_sv_col[p]];\n"
-            "    rhs[row] = acc * lu[pivot];\n  }\n}"
+            + ("    for (int p = mdx_sv_row[i + 1] - 1; p > pivot; --p) acc -= lu[p] * rhs[mdx_sv_col[p]];\n"
+               if fast else
+               "    for (int p = pivot + 1; p < mdx_sv_row[i + 1]; ++p) acc -= lu[p] * rhs[mdx_sv_col[p]];\n")
+            + "    rhs[row] = acc * lu[pivot];\n  }\n}"
         )
         out.append(
             "template <typename T, class LU, class R> __device__ __forceinline__ void mdx_sparse_solve_t(const LU& lu, R& rhs) {\n"

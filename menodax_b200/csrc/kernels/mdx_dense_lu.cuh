@@ -229,11 +229,13 @@ __device__ __forceinline__ void dense_solve_fast(const LU& lu, const IP& perm, R
     for (int j = 0; j < i; ++j) acc -= lu[i * N + j] * x[j];
     x[i] = acc;
   }
+  // Back substitution takes each row's terms latest-solved last (descending
+  // column), so a row waits on one FMA after its last input.
 #pragma unroll
   for (int i = N - 1; i >= 0; --i) {
     T acc = x[i];
 #pragma unroll
-    for (int j = i + 1; j < N; ++j) acc -= lu[i * N + j] * x[j];
+    for (int j = N - 1; j > i; --j) acc -= lu[i * N + j] * x[j];
     x[i] = acc * lu[i * N + i];
   }
 #pragma unroll

@@ -1,0 +1,148 @@
+"""The solver kernels' step code, compiled for the host and run against the oracle.
+
+`build_source` emits the whole problem source the GPU compiles: sizes, the
+traced right-hand side and Jacobian writers, the LU routines and the solver's
+init / running / step / finish.  Here that source, without its launch entry
+(`mdx_entry.cuh`), is compiled with g++ under a prelude that maps the CUDA
+spellings to host ones, and a loop of the plain kernel's shape (one trajectory
+after another: init, step while running, finish) fills the same output buffers.
+The result is held to the GPU parity bar against the oracle -- step counts
+identical on at least 99% of trajectories, saved states within 1e-9 -- so the
+kernel logic of the FP64 path is checked on every CPU run.  Both sides are
+compiled with the same FMA contraction setting (measured: identical step counts
+on every trajectory, states within 2.5e-10 for Rodas5P and 1.2e-13 for Tsit5;
+not bitwise, as the two sources contract different expressions).
+"""
+
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+from menodax_b200 import systems
+from menodax_b200._native import KERNEL_DIR
+from menodax_b200._problem import KernelOptions, build_source
+from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparsity import normalize_sparsity
+
+PRELUDE = """
+#include <cmath>
+#include <cstring>
+using std::fabs; using std::sqrt; using std::pow; using std::exp; using std::log; using std::sin;
+using std::cos; using std::tanh; using std::atan2; using std::log1p; using std::expm1;
+using std::isnan; using std::isfinite; using std::fma;
+#define __device__
+#define __host__
+#define __global__
+#define __forceinline__ inline
+#define __noinline__
+#define __restrict__
+#define __constant__
+static inline float host_fdividef(float a, float b) { return a / b; }
+static inline float host_powf(float a, float b) { return std::pow(a, b); }
+#define __fdividef host_fdividef
+#define __powf host_powf
+static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
+"""
+
+DRIVER = """
+extern "C" void run(MdxSolveArgs a) {
+  for (int i = 0; i < a.n_traj; ++i) {
+    MDX_SOLVER::State st;
+    MDX_SOLVER::init(st, a, i);
+    while (MDX_SOLVER::running(st, a)) MDX_SOLVER::step(st, a);
+    MDX_SOLVER::finish(st, a);
+  }
+}
+"""
+
+
+class Args(ctypes.Structure):
+    """MdxSolveArgs (mdx_args.h), field for field."""
+
+    _fields_ = [("y0", ctypes.c_void_p), ("times", ctypes.c_void_p), ("params", ctypes.c_void_p),
+                ("weights", ctypes.c_void_p), ("hist", ctypes.c_void_p), ("accepted", ctypes.c_void_p),
+                ("rejected", ctypes.c_void_p), ("loop_steps", ctypes.c_void_p), ("status", ctypes.c_void_p),
+                ("hook_out", ctypes.c_void_p), ("work_counter", ctypes.c_void_p), ("order", ctypes.c_void_p),
+                ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p), ("ckpt_capacity", ctypes.c_longlong),
+                ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int), ("n_save_hist", ctypes.c_int),
+                ("max_steps", ctypes.c_int), ("dt0", ctypes.c_double), ("rtol", ctypes.c_double),
+                ("atol", ctypes.c_double)]
+
+
+def _host_kernel(tmp_path, name, fn, n_vars, n_params, options):
+    from oracle.oracle import FMA
+
+    source, _ = build_source(fn, n_vars, n_params, options)
+    source = source.replace('#include "mdx_entry.cuh"', "")
+    cpp = tmp_path / f"{name}.cpp"
+    so = tmp_path / f"{name}.so"
+    cpp.write_text(PRELUDE + source + DRIVER)
+    flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}", str(cpp),
+                    "-o", str(so)], check=True)
+    lib = ctypes.CDLL(str(so))
+    lib.run.argtypes = [Args]
+    return lib
+
+
+def _solve(lib, y0, times, params, rtol, atol, max_steps=100000):
+    y0 = np.ascontiguousarray(y0, dtype=np.float64)
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    n, n_vars = y0.shape
+    hist = np.zeros((n, len(times), n_vars))
+    counters = np.zeros((4, n), dtype=np.int32)
+    a = Args()
+    a.y0, a.times, a.params = y0.ctypes.data, times.ctypes.data, params.ctypes.data
+    a.hist = hist.ctypes.data
+    a.accepted, a.rejected = counters[0].ctypes.data, counters[1].ctypes.data
+    a.loop_steps, a.status = counters[2].ctypes.data, counters[3].ctypes.data
+    a.n_traj, a.n_save, a.n_save_hist = n, len(times), len(times)
+    a.max_steps, a.dt0, a.rtol, a.atol = max_steps, 0.0, rtol, atol
+    lib.run(a)
+    return hist, counters
+
+
+def _agree(hist, counters, ref):
+    h, acc, rej, _ = ref
+    same = (counters[0] == acc) & (counters[1] == rej)
+    assert same.mean() >= 0.99
+    np.testing.assert_allclose(hist[same], h[same], rtol=1e-9, atol=1e-12)
+
+
+def test_rodas5p_robertson_fp64(tmp_path, oracle):
+    cfg = systems.robertson_config(size=64)
+    lib = _host_kernel(tmp_path, "rob", cfg["ode_fn"], 3, 3, KernelOptions(lu_precision="fp64"))
+    hist, counters = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+    ref = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
+                       rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    _agree(hist, counters, ref)
+
+
+@pytest.mark.parametrize("layout", ["dense", "sparse"])
+def test_rodas5p_vdp_ring_fp64(tmp_path, oracle, layout):
+    n_osc = 4
+    cfg = systems.vdp_ring_config(n_osc, size=64)
+    t_span = np.linspace(0.0, 30.0, 10)
+    pattern = normalize_sparsity(cfg["sparsity"], 2 * n_osc) if layout == "sparse" else None
+    lib = _host_kernel(tmp_path, f"vdp_{layout}", cfg["ode_fn"], 2 * n_osc, 1,
+                       KernelOptions(lu_precision="fp64", sparsity=pattern))
+    hist, counters = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
+    kw = {}
+    if pattern is not None:
+        solver = sparse_direct_solver_for(pattern, "amd")
+        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.compressed.colour, order=solver.layout.order)
+    ref = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span, cfg["params"],
+                       rtol=1e-6, atol=1e-8, lu_precision="fp64", **kw)
+    _agree(hist, counters, ref)
+
+
+def test_tsit5_lorenz(tmp_path, oracle):
+    cfg = systems.lorenz_config(size=64)
+    lib = _host_kernel(tmp_path, "lorenz", cfg["ode_fn"], 3, 1, KernelOptions(solver="tsit5"))
+    hist, counters = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+    ref = oracle.solve("tsit5", oracle.System.lorenz(), cfg["y0"], cfg["t_span"], cfg["params"],
+                       rtol=cfg["rtol"], atol=cfg["atol"])
+    _agree(hist, counters, ref)

@@ -146,3 +146,37 @@ def test_tsit5_lorenz(tmp_path, oracle):
     ref = oracle.solve("tsit5", oracle.System.lorenz(), cfg["y0"], cfg["t_span"], cfg["params"],
                        rtol=cfg["rtol"], atol=cfg["atol"])
     _agree(hist, counters, ref)
+
+
+@pytest.mark.parametrize("layout", ["dense", "sparse"])
+def test_rodas5p_fast_fp32_within_10_rtol(tmp_path, oracle, layout):
+    """The fast path's logic (squared-norm controller, Newton-refined reciprocals,
+    shared dense-output weights, latest-solved-last back substitution) on the
+    host: within 10 rtol of an rtol = 1e-12 oracle on Robertson, and as accurate
+    as the FP64-LU solve on the VdP ring."""
+    if layout == "dense":
+        cfg = systems.robertson_config(size=64)
+        lib = _host_kernel(tmp_path, "rob32", cfg["ode_fn"], 3, 3, KernelOptions(lu_precision="fp32", fast=True))
+        hist, _ = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+        ref, *_ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
+                               rtol=1e-12, atol=1e-16, lu_precision="fp64")
+        err = np.abs(hist - ref) / (np.abs(ref) + cfg["atol"] / cfg["rtol"])
+        assert err.max() <= 10 * cfg["rtol"]
+        return
+    n_osc = 4
+    cfg = systems.vdp_ring_config(n_osc, size=64)
+    t_span = np.linspace(0.0, 30.0, 10)
+    pattern = normalize_sparsity(cfg["sparsity"], 2 * n_osc)
+    lib = _host_kernel(tmp_path, "vdp32", cfg["ode_fn"], 2 * n_osc, 1,
+                       KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern))
+    hist, _ = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
+    system = oracle.System.vdp_ring(n_osc, 1.0, 0.1)
+    ref, *_ = oracle.solve("rodas5P", system, cfg["y0"], t_span, cfg["params"], rtol=1e-12, atol=1e-14,
+                           lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, cfg["y0"], t_span, cfg["params"], rtol=1e-6, atol=1e-8,
+                           lu_precision="fp64")
+    scale = np.abs(ref) + 1e-8 / 1e-6
+    err32 = (np.abs(hist - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    assert np.median(err32) <= 1.5 * np.median(err64) + 1e-5
+    assert err32.max() <= 3.0 * err64.max()

@@ -253,6 +253,9 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
     ``1.0 / lu[pivot]``, ``modax/_sparse_direct.py:520, 545``).  ``mode`` is
     ``"auto"`` (straight-line below the size thresholds), ``"unrolled"`` or
     ``"tables"``; the two forms perform the same operations in the same order.
+    ``fast`` (the FP32-LU product path, held to accuracy rather than to the
+    reference's bits) takes the reciprocal pivot in ``T`` with ``mdx::fast_recip``
+    and subtracts each back-substitution row's terms latest-solved last.
     """
     if mode not in ("auto", "unrolled", "tables"):
         raise ValueError(f"sparse code mode must be 'auto', 'unrolled' or 'tables'; got {mode!r}")

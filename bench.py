@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only the tuned timed launches (for ncu captures); prints no bench line")
+    ap.add_argument("--max-steps", type=int, default=100000,
+                    help="--config runs: step cap per trajectory (the solvers' default 100000); "
+                         "lower caps split a makespan into its device-full and tail parts")
     ap.add_argument("--launch", default="auto", choices=["auto", "plain", "persistent"],
                     help="launch of the timed kernel (auto = autotuned)")
     ap.add_argument("--config", default="robertson",
@@ -405,7 +408,7 @@ def run_config(args):
     params = torch.as_tensor(cfg["params"], device=dev).contiguous()
     times = torch.as_tensor(cfg["t_span"], device=dev).contiguous()
     common = dict(y0=y0, times=times, params=params, weights=None, dt0=0.0, rtol=cfg["rtol"],
-                  atol=cfg["atol"], max_steps=100000)
+                  atol=cfg["atol"], max_steps=args.max_steps)
     stream = torch.cuda.current_stream(dev)
     results = {}
     stats = None
@@ -471,7 +474,8 @@ def run_config(args):
                "cores": oracle.max_threads(), "kind": "port", "sample": f"first {sample} trajectories"}
     if rank == 0:
         print(json.dumps({"config": args.config, "trajectories": n * world, "n_vars": n_vars,
-                          "variants": results, "step_stats": stats, "cpu_baseline": cpu}))
+                          "max_steps": args.max_steps, "variants": results, "step_stats": stats,
+                          "cpu_baseline": cpu}))
 
 
 # --------------------------------------------------------------------------- our arm

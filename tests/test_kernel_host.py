@@ -180,3 +180,117 @@ def test_rodas5p_fast_fp32_within_10_rtol(tmp_path, oracle, layout):
     err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
     assert np.median(err32) <= 1.5 * np.median(err64) + 1e-5
     assert err32.max() <= 3.0 * err64.max()
+
+
+# --- the discrete adjoint -------------------------------------------------------------
+GRAD_PRELUDE = """
+struct HostDim { unsigned x, y, z; };
+static HostDim threadIdx, blockIdx, blockDim;
+#define __launch_bounds__(...)
+"""
+
+GRAD_DRIVER = """
+extern "C" void run_grad(MdxGradArgs g) {
+  blockIdx.x = 0; blockDim.x = 1;
+  for (int i = 0; i < g.n_traj; ++i) { threadIdx.x = (unsigned)i; mdx_grad_reverse(g); }
+}
+"""
+
+
+class GradArgs(ctypes.Structure):
+    """MdxGradArgs (mdx_args.h), field for field."""
+
+    _fields_ = [("times", ctypes.c_void_p), ("params", ctypes.c_void_p), ("ckpt", ctypes.c_void_p),
+                ("ckpt_count", ctypes.c_void_p), ("grad_hist", ctypes.c_void_p), ("grad_y0", ctypes.c_void_p),
+                ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p), ("order", ctypes.c_void_p),
+                ("ckpt_capacity", ctypes.c_longlong), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int),
+                ("pad", ctypes.c_int)]
+
+
+def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
+    from oracle.oracle import FMA
+
+    source, _ = build_source(fn, n_vars, n_params, options)
+    source = source.replace('#include "mdx_entry.cuh"', "")
+    cpp = tmp_path / f"{name}.cpp"
+    so = tmp_path / f"{name}.so"
+    cpp.write_text(PRELUDE + GRAD_PRELUDE + source + DRIVER + GRAD_DRIVER)
+    flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}", str(cpp),
+                    "-o", str(so)], check=True)
+    lib = ctypes.CDLL(str(so))
+    lib.run.argtypes = [Args]
+    lib.run_grad.argtypes = [GradArgs]
+    return lib
+
+
+def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity):
+    """Checkpointing forward pass, then the reverse sweep of sum(w * hist)."""
+    y0 = np.ascontiguousarray(y0, dtype=np.float64)
+    times = np.ascontiguousarray(times, dtype=np.float64)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    n, n_vars = y0.shape
+    segments = -(-capacity // stride)
+    ckpt = np.zeros(capacity * n + segments * n * (n_vars + 1))
+    ckpt_count = np.zeros(n, dtype=np.int32)
+    hist = np.zeros((n, len(times), n_vars))
+    counters = np.zeros((4, n), dtype=np.int32)
+    a = Args()
+    a.y0, a.times, a.params = y0.ctypes.data, times.ctypes.data, params.ctypes.data
+    a.hist = hist.ctypes.data
+    a.accepted, a.rejected = counters[0].ctypes.data, counters[1].ctypes.data
+    a.loop_steps, a.status = counters[2].ctypes.data, counters[3].ctypes.data
+    a.ckpt, a.ckpt_count, a.ckpt_capacity = ckpt.ctypes.data, ckpt_count.ctypes.data, capacity
+    a.n_traj, a.n_save, a.n_save_hist = n, len(times), len(times)
+    a.max_steps, a.dt0, a.rtol, a.atol = 100000, 0.0, rtol, atol
+    lib.run(a)
+    assert (counters[3] == 0).all()
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    grad_y0 = np.zeros((n, n_vars))
+    grad_p = np.zeros((n, params.shape[1]))
+    status = np.zeros(n, dtype=np.int32)
+    g = GradArgs()
+    g.times, g.params, g.ckpt, g.ckpt_count = times.ctypes.data, params.ctypes.data, ckpt.ctypes.data, \
+        ckpt_count.ctypes.data
+    g.grad_hist, g.grad_y0, g.grad_params, g.status = w.ctypes.data, grad_y0.ctypes.data, grad_p.ctypes.data, \
+        status.ctypes.data
+    g.ckpt_capacity, g.n_traj, g.n_save = capacity, n, len(times)
+    lib.run_grad(g)
+    assert (status == 0).all()
+    return hist, grad_y0, grad_p
+
+
+def _oracle_sens_grads(oracle, solver, system, y0, times, params, w, **kw):
+    """The oracle's forward sensitivities (no error control on them) contracted with w."""
+    n_vars = system.n
+    hist, *_ = oracle.solve(solver, system, y0, times, params, sens=(True, list(range(system.np)), False), **kw)
+    sens = hist[:, :, n_vars:].reshape(hist.shape[0], hist.shape[1], n_vars + system.np, n_vars)
+    g = np.einsum("nsj,nskj->nk", w, sens)
+    return hist[:, :, :n_vars], g[:, :n_vars], g[:, n_vars:]
+
+
+@pytest.mark.parametrize("stride", [1, 8])
+@pytest.mark.parametrize("solver", ["rodas5P", "tsit5"])
+def test_adjoint_matches_oracle_forward_sensitivities(tmp_path, oracle, solver, stride):
+    """The reverse sweep (segment replay, stage recompute, transposed solves,
+    VJPs and Hessian-vector products) on the host, against the oracle's forward
+    sensitivities on the same step sequence: the two are transposes of one linear
+    map, so they agree to rounding (the GPU tests' bar, 1e-7 of the largest)."""
+    if solver == "rodas5P":
+        cfg = systems.robertson_config(size=32)
+        system, n_vars, n_params, kw = oracle.System.robertson(), 3, 3, dict(lu_precision="fp64")
+        options = KernelOptions(lu_precision="fp64", checkpoint=True, adjoint=True, ckpt_stride=stride)
+    else:
+        cfg = systems.lorenz_config(size=32)
+        system, n_vars, n_params, kw = oracle.System.lorenz(), 3, 1, {}
+        options = KernelOptions(solver="tsit5", checkpoint=True, adjoint=True, ckpt_stride=stride)
+    lib = _host_adjoint(tmp_path, f"adj_{solver}_{stride}", cfg["ode_fn"], n_vars, n_params, options)
+    w = np.random.default_rng(4).normal(size=(32, len(cfg["t_span"]), n_vars))
+    hist, gy, gp = _value_and_grad(lib, cfg["y0"], cfg["t_span"], cfg["params"], w, cfg["rtol"], cfg["atol"],
+                                   stride, capacity=4096)
+    oh, oy, op = _oracle_sens_grads(oracle, solver, system, cfg["y0"], cfg["t_span"], cfg["params"], w,
+                                    rtol=cfg["rtol"], atol=cfg["atol"], **kw)
+    np.testing.assert_allclose(hist, oh, rtol=1e-9, atol=1e-14)
+    for got, ref in ((gy, oy), (gp, op)):
+        scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
+        assert (np.abs(got - ref) / scale).max() < 1e-7

@@ -47,13 +47,14 @@ static inline double __longlong_as_double(long long x) { double d; std::memcpy(&
 """
 
 DRIVER = """
-extern "C" void run(MdxSolveArgs a) {
+extern "C" int run(MdxSolveArgs a) {
   for (int i = 0; i < a.n_traj; ++i) {
     MDX_SOLVER::State st;
     MDX_SOLVER::init(st, a, i);
     while (MDX_SOLVER::running(st, a)) MDX_SOLVER::step(st, a);
     MDX_SOLVER::finish(st, a);
   }
+  return 0;
 }
 """
 
@@ -84,6 +85,7 @@ def _host_kernel(tmp_path, name, fn, n_vars, n_params, options):
                     "-o", str(so)], check=True)
     lib = ctypes.CDLL(str(so))
     lib.run.argtypes = [Args]
+    lib.run.restype = ctypes.c_int
     return lib
 
 
@@ -101,7 +103,7 @@ def _solve(lib, y0, times, params, rtol, atol, max_steps=100000):
     a.loop_steps, a.status = counters[2].ctypes.data, counters[3].ctypes.data
     a.n_traj, a.n_save, a.n_save_hist = n, len(times), len(times)
     a.max_steps, a.dt0, a.rtol, a.atol = max_steps, 0.0, rtol, atol
-    lib.run(a)
+    assert lib.run(a) == 0
     return hist, counters
 
 
@@ -220,6 +222,7 @@ def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
                     "-o", str(so)], check=True)
     lib = ctypes.CDLL(str(so))
     lib.run.argtypes = [Args]
+    lib.run.restype = ctypes.c_int
     lib.run_grad.argtypes = [GradArgs]
     return lib
 
@@ -243,7 +246,7 @@ def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity):
     a.ckpt, a.ckpt_count, a.ckpt_capacity = ckpt.ctypes.data, ckpt_count.ctypes.data, capacity
     a.n_traj, a.n_save, a.n_save_hist = n, len(times), len(times)
     a.max_steps, a.dt0, a.rtol, a.atol = 100000, 0.0, rtol, atol
-    lib.run(a)
+    assert lib.run(a) == 0
     assert (counters[3] == 0).all()
     w = np.ascontiguousarray(w, dtype=np.float64)
     grad_y0 = np.zeros((n, n_vars))

@@ -1,0 +1,212 @@
+"""The team kernel, compiled for the host with its lanes as threads.
+
+The team kernel (one trajectory per team of 4-32 lanes, its vectors and matrix
+in a shared-memory slice) keeps every lane of a team on the same path, so its
+warp intrinsics can be emulated lane by lane: `__syncwarp` is a barrier over
+the team's lanes, a shuffle writes the lane's value to an
+exchange slot, meets the team at the barrier, reads the source lane's slot and
+meets it again, and `__any_sync` is the same with an OR.  Lanes are
+user-level contexts on one host thread, switched at every barrier; the block's
+dynamic shared memory is one host buffer; blocks run one after another.  The kernel
+source is exactly what the GPU compiles (`build_source`), so this checks the
+team code -- class loops, panel LU, blocked solves, the first lane's sparse
+solves, the error norm and the controller -- on every CPU run, against the
+oracle and the thread kernel compiled the same way.
+"""
+
+import ctypes
+import subprocess
+
+import numpy as np
+import pytest
+
+from menodax_b200 import systems
+from menodax_b200._native import KERNEL_DIR
+from menodax_b200._problem import KernelOptions, build_source
+from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparsity import normalize_sparsity
+
+from test_kernel_host import PRELUDE, Args, _host_kernel, _solve
+
+LANES = """
+#include <ucontext.h>
+#include <cstdio>
+#include <cstdlib>
+struct HostDim { unsigned x, y, z; };
+static HostDim threadIdx, blockIdx, blockDim;
+static unsigned host_lane;
+static int host_team_size = 32;
+
+// Lanes are user-level contexts on one OS thread: a lane runs until it reaches
+// a barrier or ends, then the scheduler runs the next; a team's lanes leave the
+// barrier together once every lane of the team that has not ended waits there.
+struct HostLane { ucontext_t ctx; bool done, waiting; };
+static HostLane host_lanes[32];
+static ucontext_t host_scheduler;
+static unsigned long long host_slot[32];
+
+static inline void __syncwarp(unsigned = 0xffffffffu) {
+  host_lanes[host_lane].waiting = true;
+  swapcontext(&host_lanes[host_lane].ctx, &host_scheduler);
+}
+template <class T> static inline T host_exchange(T v, unsigned src) {
+  std::memcpy(&host_slot[host_lane], &v, sizeof(T));
+  __syncwarp();
+  T r;
+  std::memcpy(&r, &host_slot[src], sizeof(T));
+  __syncwarp();
+  return r;
+}
+template <class T> static inline T __shfl_xor_sync(unsigned, T v, int off, int width = 32) {
+  const unsigned base = host_lane & ~(unsigned)(width - 1);
+  return host_exchange(v, base | ((host_lane - base) ^ (unsigned)off));
+}
+template <class T> static inline T __shfl_sync(unsigned, T v, int src, int width = 32) {
+  const unsigned base = host_lane & ~(unsigned)(width - 1);
+  return host_exchange(v, base + ((unsigned)src & (unsigned)(width - 1)));
+}
+static inline bool __any_sync(unsigned mask, bool p) {
+  host_slot[host_lane] = p ? 1ull : 0ull;
+  __syncwarp();
+  bool r = false;
+  for (unsigned l = 0; l < 32; ++l) if ((mask >> l) & 1u) r = r || host_slot[l] != 0ull;
+  __syncwarp();
+  return r;
+}
+static inline int atomicAdd(int* p, int v) { const int o = *p; *p += v; return o; }
+#define __shared__
+#define __align__(n)
+#define __launch_bounds__(...)
+namespace mdx { namespace team { alignas(16) unsigned char mdx_team_smem[1 << 20]; } }
+"""
+
+DRIVER = """
+static MdxSolveArgs host_args;
+static void host_lane_main() {
+  mdx_solve_plain(host_args);
+  host_lanes[host_lane].done = true;
+}
+
+extern "C" int run(MdxSolveArgs a) {
+  static char stacks[MDX_TPB][1 << 18];
+  host_args = a;
+  host_team_size = MDX_TEAM;
+  blockDim.x = MDX_TPB;
+  const int per_block = MDX_TPB / MDX_TEAM;
+  const int blocks = (a.n_traj + per_block - 1) / per_block;
+  for (int b = 0; b < blocks; ++b) {
+    blockIdx.x = (unsigned)b;
+    for (int l = 0; l < MDX_TPB; ++l) {
+      HostLane& h = host_lanes[l];
+      h.done = h.waiting = false;
+      getcontext(&h.ctx);
+      h.ctx.uc_stack.ss_sp = stacks[l];
+      h.ctx.uc_stack.ss_size = sizeof(stacks[l]);
+      h.ctx.uc_link = &host_scheduler;
+      makecontext(&h.ctx, host_lane_main, 0);
+    }
+    for (;;) {
+      bool live = false;
+      for (int l = 0; l < MDX_TPB; ++l) {
+        if (host_lanes[l].done || host_lanes[l].waiting) continue;
+        host_lane = (unsigned)l;
+        threadIdx.x = (unsigned)l;
+        swapcontext(&host_scheduler, &host_lanes[l].ctx);
+      }
+      for (int t = 0; t < MDX_TPB / MDX_TEAM; ++t) {
+        int waiting = 0, done = 0;
+        for (int l = t * MDX_TEAM; l < (t + 1) * MDX_TEAM; ++l) {
+          waiting += host_lanes[l].waiting;
+          done += host_lanes[l].done;
+        }
+        if (waiting && done) return 1;  // a lane ended while its team waits: divergent code
+        if (waiting == MDX_TEAM)
+          for (int l = t * MDX_TEAM; l < (t + 1) * MDX_TEAM; ++l) host_lanes[l].waiting = false;
+        live = live || done < MDX_TEAM;
+      }
+      if (!live) break;
+    }
+  }
+  return 0;
+}
+"""
+
+
+def _team_kernel(tmp_path, name, fn, n_vars, n_params, options):
+    from oracle.oracle import FMA
+
+    source, meta = build_source(fn, n_vars, n_params, options)
+    assert meta["shared_bytes"] <= 1 << 20
+    cpp = tmp_path / f"{name}.cpp"
+    so = tmp_path / f"{name}.so"
+    cpp.write_text(PRELUDE + LANES + source + DRIVER)
+    flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}",
+                    str(cpp), "-o", str(so)], check=True)
+    lib = ctypes.CDLL(str(so))
+    lib.run.argtypes = [Args]
+    lib.run.restype = ctypes.c_int
+    return lib
+
+
+def _same_steps_and_states(hist, counters, h, acc, rej, rtol=1e-9, atol=1e-12):
+    same = (counters[0] == acc) & (counters[1] == rej)
+    assert same.mean() >= 0.99
+    np.testing.assert_allclose(hist[same], h[same], rtol=rtol, atol=atol)
+
+
+@pytest.mark.parametrize("team", [4, 8])
+@pytest.mark.parametrize("layout", ["sparse", "dense"])
+def test_team_vdp_ring_fp64_matches_oracle(tmp_path, oracle, team, layout):
+    """The GPU test of the same name on the host: FP64, both layouts."""
+    n_osc = 4
+    cfg = systems.vdp_ring_config(n_osc, size=16)
+    t_span = np.linspace(0.0, 30.0, 10)
+    pattern = normalize_sparsity(cfg["sparsity"], 2 * n_osc) if layout == "sparse" else None
+    lib = _team_kernel(tmp_path, f"team_{layout}_{team}", cfg["ode_fn"], 2 * n_osc, 1,
+                       KernelOptions(lu_precision="fp64", sparsity=pattern, team=team, threads_per_block=32))
+    hist, counters = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
+    kw = {}
+    if pattern is not None:
+        solver = sparse_direct_solver_for(pattern, "amd")
+        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.compressed.colour, order=solver.layout.order)
+    h, acc, rej, _ = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span,
+                                  cfg["params"], rtol=1e-6, atol=1e-8, lu_precision="fp64", **kw)
+    _same_steps_and_states(hist, counters, h, acc, rej)
+
+
+@pytest.mark.parametrize("n_osc", [5, 6])
+def test_team_dense_panels_factor_like_the_thread_kernel(tmp_path, n_osc):
+    """The GPU panel test on the host: fast FP64 arithmetic, four-column panels on
+    4 lanes (10 states end on a two-column panel), against the thread kernel's
+    register LU compiled the same way."""
+    cfg = systems.vdp_ring_config(n_osc, size=16)
+    t_span = np.linspace(0.0, 30.0, 10)
+    n = 2 * n_osc
+    team = _team_kernel(tmp_path, f"panel_{n}", cfg["ode_fn"], n, 1,
+                        KernelOptions(lu_precision="fp64", fast=True, team=4, threads_per_block=32))
+    thread = _host_kernel(tmp_path, f"thread_{n}", cfg["ode_fn"], n, 1, KernelOptions(lu_precision="fp64", fast=True))
+    h4, c4 = _solve(team, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
+    h0, c0 = _solve(thread, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
+    _same_steps_and_states(h4, c4, h0, c0[0], c0[1], atol=1e-9)
+
+
+@pytest.mark.parametrize("team", [8, 16])
+def test_team_brusselator_dense_fp32_as_accurate_as_fp64(tmp_path, oracle, team):
+    """Fast FP32 dense LU with four-column panels (16 states: 8 lanes hold two
+    pivot-row entries each, 16 lanes one) on a smooth system."""
+    n_grid = 8
+    cfg = systems.brusselator_config(n_grid=n_grid, size=16)
+    lib = _team_kernel(tmp_path, f"bruss_{team}", cfg["ode_fn"], 2 * n_grid, 1,
+                       KernelOptions(lu_precision="fp32", fast=True, team=team, threads_per_block=32))
+    h32, _ = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+    system = oracle.System.brusselator(n_grid)
+    ref, *_ = oracle.solve("rodas5P", system, cfg["y0"], cfg["t_span"], cfg["params"], rtol=1e-12, atol=1e-14,
+                           lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, cfg["y0"], cfg["t_span"], cfg["params"], rtol=cfg["rtol"],
+                           atol=cfg["atol"], lu_precision="fp64")
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    err32 = (np.abs(h32 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    assert np.median(err32) <= 1.5 * np.median(err64) + 10 * cfg["rtol"]
+    assert err32.max() <= 3.0 * err64.max()

@@ -49,6 +49,7 @@ static inline double __longlong_as_double(long long x) { double d; std::memcpy(&
 DRIVER = """
 extern "C" int run(MdxSolveArgs a) {
   for (int i = 0; i < a.n_traj; ++i) {
+    MDX_HOST_THREAD(i);
     MDX_SOLVER::State st;
     MDX_SOLVER::init(st, a, i);
     while (MDX_SOLVER::running(st, a)) MDX_SOLVER::step(st, a);
@@ -72,6 +73,16 @@ class Args(ctypes.Structure):
                 ("atol", ctypes.c_double)]
 
 
+# Thread-kernel builds run trajectory i as thread i % MDX_TPB of its block, for
+# code that keeps a per-thread column of a block's shared array.
+THREAD_DIMS = """
+struct HostDim { unsigned x, y, z; };
+static HostDim threadIdx, blockIdx, blockDim;
+#define __shared__ static
+#define MDX_HOST_THREAD(i) (threadIdx.x = (unsigned)((i) % MDX_TPB))
+"""
+
+
 def _host_kernel(tmp_path, name, fn, n_vars, n_params, options):
     from oracle.oracle import FMA
 
@@ -79,7 +90,7 @@ def _host_kernel(tmp_path, name, fn, n_vars, n_params, options):
     source = source.replace('#include "mdx_entry.cuh"', "")
     cpp = tmp_path / f"{name}.cpp"
     so = tmp_path / f"{name}.so"
-    cpp.write_text(PRELUDE + source + DRIVER)
+    cpp.write_text(PRELUDE + THREAD_DIMS + source + DRIVER)
     flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
     subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}", str(cpp),
                     "-o", str(so)], check=True)
@@ -142,12 +153,18 @@ def test_rodas5p_vdp_ring_fp64(tmp_path, oracle, layout):
 
 
 def test_tsit5_lorenz(tmp_path, oracle):
+    """Both stage placements (registers; a per-thread column of a shared array,
+    the reference's shared backend): the same arithmetic, so bit for bit."""
     cfg = systems.lorenz_config(size=64)
-    lib = _host_kernel(tmp_path, "lorenz", cfg["ode_fn"], 3, 1, KernelOptions(solver="tsit5"))
-    hist, counters = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+    out = {}
+    for shared in (False, True):
+        lib = _host_kernel(tmp_path, f"lorenz_{int(shared)}", cfg["ode_fn"], 3, 1,
+                           KernelOptions(solver="tsit5", shared_stages=shared))
+        out[shared] = _solve(lib, cfg["y0"], cfg["t_span"], cfg["params"], cfg["rtol"], cfg["atol"])
+    assert np.array_equal(out[False][0], out[True][0]) and np.array_equal(out[False][1], out[True][1])
     ref = oracle.solve("tsit5", oracle.System.lorenz(), cfg["y0"], cfg["t_span"], cfg["params"],
                        rtol=cfg["rtol"], atol=cfg["atol"])
-    _agree(hist, counters, ref)
+    _agree(*out[False], ref)
 
 
 @pytest.mark.parametrize("layout", ["dense", "sparse"])
@@ -186,8 +203,6 @@ def test_rodas5p_fast_fp32_within_10_rtol(tmp_path, oracle, layout):
 
 # --- the discrete adjoint -------------------------------------------------------------
 GRAD_PRELUDE = """
-struct HostDim { unsigned x, y, z; };
-static HostDim threadIdx, blockIdx, blockDim;
 #define __launch_bounds__(...)
 """
 
@@ -216,7 +231,7 @@ def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
     source = source.replace('#include "mdx_entry.cuh"', "")
     cpp = tmp_path / f"{name}.cpp"
     so = tmp_path / f"{name}.so"
-    cpp.write_text(PRELUDE + GRAD_PRELUDE + source + DRIVER + GRAD_DRIVER)
+    cpp.write_text(PRELUDE + THREAD_DIMS + GRAD_PRELUDE + source + DRIVER + GRAD_DRIVER)
     flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
     subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}", str(cpp),
                     "-o", str(so)], check=True)

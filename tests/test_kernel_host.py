@@ -312,3 +312,29 @@ def test_adjoint_matches_oracle_forward_sensitivities(tmp_path, oracle, solver, 
     for got, ref in ((gy, oy), (gp, op)):
         scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
         assert (np.abs(got - ref) / scale).max() < 1e-7
+
+
+def test_rodas5p_time_derivative_and_tf_index(tmp_path):
+    """The reference's tests/test_solver_options.py:40-93 on the host: df/dt reaches
+    the stages of a non-autonomous system (y' = -a y + b t, exact
+    b (a t - 1 + exp(-a t)) / a^2), and tf_index ends each trajectory at its own
+    time with the later saves frozen."""
+    t_span = np.linspace(0.0, 1.0, 11)
+    params = np.array([[10.0, 5.0, 1.0], [10.0, 5.0, 0.5]])
+    lib = _host_kernel(tmp_path, "forced", systems.forced_decay, 1, 3,
+                       KernelOptions(lu_precision="fp64", tf_index=2))
+    a = Args()
+    y0 = np.zeros((2, 1))
+    hist = np.zeros((2, len(t_span), 1))
+    counters = np.zeros((4, 2), dtype=np.int32)
+    a.y0, a.times, a.params, a.hist = y0.ctypes.data, t_span.ctypes.data, params.ctypes.data, hist.ctypes.data
+    a.accepted, a.rejected = counters[0].ctypes.data, counters[1].ctypes.data
+    a.loop_steps, a.status = counters[2].ctypes.data, counters[3].ctypes.data
+    a.n_traj, a.n_save, a.n_save_hist = 2, len(t_span), len(t_span)
+    a.max_steps, a.dt0, a.rtol, a.atol = 100000, 1e-4, 1e-10, 1e-12
+    assert lib.run(a) == 0
+    exact = 5.0 * (10.0 * t_span - 1.0 + np.exp(-10.0 * t_span)) / 100.0
+    np.testing.assert_allclose(hist[0, :, 0], exact, rtol=1e-8, atol=1e-10)
+    stops = int(np.searchsorted(t_span, 0.5, side="right"))
+    np.testing.assert_allclose(hist[1, :stops, 0], exact[:stops], rtol=1e-8, atol=1e-10)
+    assert (hist[1, stops:, 0] == hist[1, stops - 1, 0]).all()

@@ -330,12 +330,12 @@ def config_roofline(fn, n_vars, n_params, opts, counters, n, n_save, launch_ms, 
     import torch
 
     from menodax_b200._flops import rodas5p_cost, tsit5_cost
-    from menodax_b200._sparse_direct import sparse_direct_solver_for
+    from menodax_b200._sparse_direct import sparse_lu_for
 
     if opts.solver == "tsit5":
         cost = tsit5_cost(fn, n_vars, n_params)
     else:
-        sparse = sparse_direct_solver_for(opts.sparsity, opts.ordering) if opts.sparsity is not None else None
+        sparse = sparse_lu_for(opts.sparsity, opts.ordering) if opts.sparsity is not None else None
         cost = rodas5p_cost(fn, n_vars, n_params, sparse=sparse)
     steps = float(counters[2].to(torch.float64).sum())
     f64 = steps * cost.f64 + n * (n_save - 1) * cost.per_save

@@ -43,7 +43,7 @@ def rodas5p_cost(ode_fn, n_vars: int, n_params: int, *, sparse=None) -> StepCost
     tr = trace(ode_fn, n_vars, n_params)
     g = tr.graph
     rhs = _ops(g, tr.outputs)
-    compressed = dense_jacobian(n_vars) if sparse is None else sparse.compressed
+    compressed = dense_jacobian(n_vars) if sparse is None else sparse.slots
     roots = []
     for colour in range(compressed.n_colours):
         seeds = {tr.y[c]: g.const(1.0) for c in range(n_vars) if compressed.colour[c] == colour}
@@ -67,7 +67,7 @@ def rodas5p_cost(ode_fn, n_vars: int, n_params: int, *, sparse=None) -> StepCost
         lu_work = 8 * solve + n
         f64 = jac + 8 * rhs + stages + advance + error + controller + factor
     else:
-        mult, upd, subs = sparse.layout.flop_counts()
+        mult, upd, subs = sparse.structure.counts()
         factor_lu = mult + 2 * upd
         solve = 2 * subs + n
         lu_work = factor_lu + 8 * solve + n

@@ -21,7 +21,7 @@ from menodax_b200._codegen import (
     emit_sens_coupling,
     lit,
 )
-from menodax_b200._sparse_direct import MAX_UNROLLED_SUBSTITUTIONS, sparse_direct_solver_for
+from menodax_b200._sparse_direct import MAX_UNROLLED_SUBSTITUTIONS, sparse_lu_for
 from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
 from menodax_b200._team import TEAM_SIZES, dense_lda, emit_team_functions
 from menodax_b200._team import slice_bytes as team_slice_bytes
@@ -112,7 +112,7 @@ def team_block_threads(n_vars: int, n_params: int, options: KernelOptions, prefe
     if dense:
         lu_size = n_vars * dense_lda(n_vars)
     else:
-        lu_size = sparse_direct_solver_for(options.sparsity, options.ordering).compressed.size
+        lu_size = sparse_lu_for(options.sparsity, options.ordering).slots.size
     per = team_slice_bytes(n_vars, n_params, lu_size, lu_bytes, dense=dense, autonomous=False,
                            fast=options.fast)
     fit = max(1, _native.MDX_MAX_SHARED_BYTES // per)
@@ -153,8 +153,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
         sparse = None
         sparse_registers = 0
     else:
-        sparse = sparse_direct_solver_for(options.sparsity, options.ordering)
-        structure = sparse.compressed
+        sparse = sparse_lu_for(options.sparsity, options.ordering)
+        structure = sparse.slots
         lu_size = structure.size
         store = structure.store_slots()
 
@@ -167,8 +167,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
         diag = ", ".join(str(int(d)) for d in structure.diagonal)
         extra.append(f"__device__ const int mdx_team_diag[{n_vars}] = {{{diag}}};")
         extra.append("__device__ __forceinline__ int mdx_team_diag_slot(int d) { return mdx_team_diag[d]; }")
-        extra.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code, fast=options.fast))
-        substitutions = sparse.layout.flop_counts()[2]
+        extra.append(emit_sparse_lu(sparse.structure, options.sparse_code, fast=options.fast))
+        substitutions = sparse.structure.counts()[2]
         sparse_registers = int(options.sparse_code == "unrolled" or (
             options.sparse_code == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS))
     slice_size = team_slice_bytes(n_vars, n_params, lu_size, lu_bytes, dense=dense,
@@ -306,12 +306,12 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 "__device__ __forceinline__ int mdx_diag_slot(int d) { return d * MDX_NV + d; }"
             )
         else:
-            sparse = sparse_direct_solver_for(options.sparsity, options.ordering)
-            structure = sparse.compressed
+            sparse = sparse_lu_for(options.sparsity, options.ordering)
+            structure = sparse.slots
             lu_size = structure.size
             parts.append(f"#define MDX_LU_SIZE {lu_size}")
             parts.append("#define MDX_IPIV 1")
-            parts.append(emit_sparse_lu(sparse.layout, sparse.ops, options.sparse_code, fast=options.fast))
+            parts.append(emit_sparse_lu(sparse.structure, options.sparse_code, fast=options.fast))
             diag = structure.diagonal
             cases = " ".join(f"case {d}: return {int(s)};" for d, s in enumerate(diag))
             parts.append(
@@ -401,4 +401,4 @@ def clear_caches() -> None:
     """Drop every compiled problem (``modax/tsit5.py:142-153``)."""
     with _cache_lock:
         _cache.clear()
-    sparse_direct_solver_for.cache_clear()
+    sparse_lu_for.cache_clear()

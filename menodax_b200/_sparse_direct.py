@@ -1,44 +1,54 @@
 """A sparse direct solver for the Rodas5P iteration matrix, compiled per pattern.
 
-Host-side analysis, once per pattern, as ``modax/_sparse_direct.py`` does it:
+The kernel's matrix ``M = I / (h gamma) - J`` has the Jacobian's pattern plus
+the diagonal.  Given that pattern (the ``sparsity`` argument, as in
+``modax/_sparse_direct.py``), the host analyses it once:
 
-1. **Order** (``fill_reducing_order``): a symmetric fill-reducing permutation of
-   ``S + S^T + I``.  ``modax`` calls SuiteSparse AMD through cvxopt
-   (``modax/_sparse_direct.py:91-152``); cvxopt is not part of this build, so the
-   ordering here is this module's own minimum-degree elimination on the
-   explicit elimination graph, with *exact* external degrees -- the quantity AMD
-   approximates.  For the tens-to-hundreds of variables these solvers take, the
-   exact graph costs milliseconds.  Ties go to the vertex with the smaller
-   original degree, then the smaller index.
-2. **Fill** (``fill_pattern``): pattern-only unpivoted Gaussian elimination gives
-   the exact ``L + U`` structure (``modax/_sparse_direct.py:155-184``).
-3. **Layout** (``analyse``/``SparseLULayout``): one CSR image of ``L + U`` in
-   elimination order, ``row_ptr``/``col_ind``/``diag_ptr``, the diagonal holding
-   ``1/U_ii`` after factorisation (``modax/_sparse_direct.py:187-349``).
-4. **Emit** (``emit_cuda``): the up-looking factorisation and the two
-   triangular solves as CUDA device code, straight-line with literal slots when
-   small (``modax/_sparse_direct.py:468-469`` thresholds), loops over
-   ``__constant__`` index tables otherwise.  The transposed solve the discrete
-   adjoint needs is emitted the same way.
+1. **Order** (``fill_reducing_order``): a symmetric fill-reducing permutation.
+   ``modax`` calls SuiteSparse AMD through cvxopt
+   (``modax/_sparse_direct.py:91-152``); cvxopt is not part of this build, so
+   ``minimum_degree_order`` eliminates on the explicit elimination graph with
+   *exact* external degrees -- the quantity AMD approximates.  For the tens to
+   hundreds of variables these solvers take the exact graph costs milliseconds.
+2. **Symbolic factorisation** (``symbolic_rows``): each row of ``L + U`` is
+   found the way the numeric factorisation will build it, up-looking -- row
+   ``i`` starts from the pattern's row plus the diagonal and absorbs the upper
+   part of every earlier row ``k`` it holds a multiplier for, smallest ``k``
+   first (a heap), since absorbing row ``k`` can only add columns right of
+   ``k``.  Without cancellation this is the exact fill of an unpivoted LU.
+3. **Structure** (``LUStructure``): the rows stored as one CSR image of
+   ``L + U`` in elimination order (``indptr``/``indices``, ``diag`` the slot of
+   each pivot, which holds ``1 / U_ii`` after factorisation), and the
+   ``UpdatePlan`` listing, per multiplier in execution order, the source and
+   destination slots of its row update.  CSR by rows, in elimination order, with
+   a reciprocal pivot, is the reference's storage (``modax/_sparse_direct.py:187-230``):
+   the Jacobian sweeps write into it, so the format decides the numbers.
+4. **Emit** (``emit_cuda``): the up-looking factorisation and the two triangular
+   solves as CUDA device code, straight-line with literal slots below the size
+   thresholds (``modax/_sparse_direct.py:468-469``), loops over ``__constant__``
+   tables otherwise.  The transposed solve the discrete adjoint needs is emitted
+   the same way.
 
-No pivoting: the permutation is symmetric so ``I/(h*gamma)`` keeps every pivot
-structurally present, and a Rosenbrock-W step tolerates an approximate
+No pivoting: the permutation is symmetric, so ``I / (h gamma)`` keeps every
+pivot structurally present, and a Rosenbrock-W step tolerates an approximate
 factorisation (``modax/_sparse_direct.py:51-61``).
 """
 
 from __future__ import annotations
 
 import functools
-from dataclasses import dataclass, replace
+import heapq
+from dataclasses import dataclass
 
 import numpy as np
 
-from menodax_b200._sparsity import CompressedJacobian, colour_sparsity, normalize_sparsity
+from menodax_b200._sparsity import SlotMap, colour_columns, normalize_sparsity
 
 ORDERINGS = ("amd", "natural")
 
 # Above these the routines are emitted as loops over constant-memory tables
-# instead of straight-line code (modax/_sparse_direct.py:468-469).
+# instead of straight-line code (the reference's thresholds,
+# modax/_sparse_direct.py:468-469).
 MAX_UNROLLED_SUBSTITUTIONS = 2048
 MAX_UNROLLED_UPDATES = 8192
 
@@ -76,167 +86,193 @@ def fill_reducing_order(pattern, ordering: str = "amd") -> tuple[int, ...]:
     return minimum_degree_order(pattern)
 
 
-def fill_pattern(pattern: tuple[tuple[int, ...], ...]) -> np.ndarray:
-    """Exact boolean ``L + U`` pattern of an unpivoted LU, diagonal included."""
-    n = len(pattern)
-    filled = np.zeros((n, n), dtype=bool)
-    for row, cols in enumerate(pattern):
-        filled[row, list(cols)] = True
-    np.fill_diagonal(filled, True)
-    for k in range(n):
-        below = np.flatnonzero(filled[k + 1:, k]) + k + 1
-        if below.size:
-            filled[below, k + 1:] |= filled[k, k + 1:]
-    return filled
+def symbolic_rows(rows: list[list[int]] | tuple[tuple[int, ...], ...]) -> list[np.ndarray]:
+    """Sorted column indices of each row of ``L + U`` (diagonal included).
+
+    ``rows`` is the matrix's pattern in elimination indices.  Row ``i`` absorbs
+    the strictly-upper structure of each row ``k < i`` in which it holds an
+    entry; popping those ``k`` from a min-heap visits them in the order the
+    numeric up-looking factorisation does, and any column a merge adds left of
+    the diagonal is pushed for a later merge.
+    """
+    n = len(rows)
+    upper: list[np.ndarray] = []
+    out: list[np.ndarray] = []
+    for i in range(n):
+        present = set(int(c) for c in rows[i])
+        present.add(i)
+        pending = [c for c in present if c < i]
+        heapq.heapify(pending)
+        while pending:
+            k = heapq.heappop(pending)
+            for c in upper[k]:
+                c = int(c)
+                if c not in present:
+                    present.add(c)
+                    if c < i:
+                        heapq.heappush(pending, c)
+        cols = np.array(sorted(present), dtype=np.int32)
+        out.append(cols)
+        upper.append(cols[cols > i])
+    return out
 
 
-@dataclass(frozen=True)
-class SparseLULayout:
-    """CSR image of ``L + U`` in elimination order (row ``i`` is variable ``order[i]``)."""
+@dataclass(frozen=True, eq=False)
+class UpdatePlan:
+    """The factorisation's row updates, one entry per multiplier in execution order.
 
-    n_vars: int
+    Multiplier ``j`` sits in slot ``mult[j]`` of row ``row[j]`` at column ``k``; it
+    is scaled by the reciprocal pivot in slot ``pivot[j]`` and then subtracts
+    ``L_ik * lu[s]`` for the sources ``s = src_begin[j] .. src_end[j] - 1`` (row
+    ``k``'s upper slots, contiguous in CSR) from the destinations
+    ``dst[dst_begin[j] + (s - src_begin[j])]`` (the same columns in row ``i``).
+    ``row_begin[i] .. row_begin[i + 1]`` are row ``i``'s multipliers.
+    """
+
+    row_begin: np.ndarray
+    mult: np.ndarray
+    pivot: np.ndarray
+    src_begin: np.ndarray
+    src_end: np.ndarray
+    dst_begin: np.ndarray
+    dst: np.ndarray
+
+    @property
+    def n_updates(self) -> int:
+        return int(self.dst.size)
+
+
+@dataclass(frozen=True, eq=False)
+class LUStructure:
+    """``L + U`` of the permuted matrix as one CSR image in elimination order.
+
+    Row ``i`` of the image is the caller's variable ``order[i]``; ``indices`` are
+    elimination indices, sorted within each row, so a row's strictly-lower slots
+    run ``indptr[i] .. diag[i] - 1`` and its upper ones ``diag[i] + 1 ..
+    indptr[i + 1] - 1``.
+    """
+
     order: tuple[int, ...]
-    row_ptr: np.ndarray
-    col_ind: np.ndarray
-    diag_ptr: np.ndarray
+    indptr: np.ndarray
+    indices: np.ndarray
+    diag: np.ndarray
+    plan: UpdatePlan
+
+    @property
+    def n_vars(self) -> int:
+        return len(self.order)
 
     @property
     def nnz(self) -> int:
-        return int(self.row_ptr[-1])
+        return int(self.indptr[-1])
 
     @property
     def row_origin(self) -> np.ndarray:
+        """Caller's index of each elimination row."""
         return np.asarray(self.order, dtype=np.int32)
 
     @property
     def col_origin(self) -> np.ndarray:
-        return np.asarray(self.order, dtype=np.int32)[self.col_ind]
+        """Caller's index of the column of each slot."""
+        return self.row_origin[self.indices]
 
-    def slot_table(self) -> np.ndarray:
-        """``(n, n)`` caller-index -> slot map, ``-1`` outside the structure."""
+    def caller_slots(self) -> np.ndarray:
+        """``(n, n)`` slot of each caller-indexed entry, ``-1`` outside ``L + U``."""
         table = np.full((self.n_vars, self.n_vars), -1, dtype=np.int64)
-        origin = np.asarray(self.order, dtype=np.int64)
-        for i in range(self.n_vars):
-            start, stop = int(self.row_ptr[i]), int(self.row_ptr[i + 1])
-            table[origin[i], origin[self.col_ind[start:stop]]] = np.arange(start, stop)
+        rows = np.repeat(self.row_origin, np.diff(self.indptr))
+        table[rows, self.col_origin] = np.arange(self.nnz)
         return table
 
-    def factorization_ops(self):
-        """``(dst_start, destination, upper_end)`` indexed by multiplier slot.
-
-        For multiplier ``p = (i, k)`` the update ``row_i -= L_ik * U_k,k+1:`` reads
-        row ``k``'s upper slots ``diag_ptr[k]+1 .. row_ptr[k+1]`` in order and
-        writes ``destination[dst_start[p] + j]`` (``modax/_sparse_direct.py:241-283``).
-        """
-        n = self.n_vars
-        dst_start = np.zeros(self.nnz, dtype=np.int64)
-        upper_end = np.asarray(self.row_ptr[1:], dtype=np.int64)[np.asarray(self.col_ind, dtype=np.int64)]
-        dst: list[int] = []
-        table = np.full((n, n), -1, dtype=np.int64)
-        for i in range(n):
-            start, stop = int(self.row_ptr[i]), int(self.row_ptr[i + 1])
-            table[i, self.col_ind[start:stop]] = np.arange(start, stop)
-        for i in range(n):
-            for p in range(int(self.row_ptr[i]), int(self.diag_ptr[i])):
-                k = int(self.col_ind[p])
-                dst_start[p] = len(dst)
-                for q in range(int(self.diag_ptr[k]) + 1, int(self.row_ptr[k + 1])):
-                    dst.append(int(table[i, int(self.col_ind[q])]))
-        return (
-            dst_start.astype(np.int32),
-            np.asarray(dst, dtype=np.int32),
-            upper_end.astype(np.int32),
-        )
-
-    def flop_counts(self) -> tuple[int, int, int]:
-        """``(multipliers, updates, substitutions)`` of one factorisation / one solve."""
-        lower = self.diag_ptr - self.row_ptr[:-1]
-        upper = self.row_ptr[1:] - self.diag_ptr - 1
-        multipliers = int(lower.sum())
-        slot = np.arange(self.nnz)
-        row = np.repeat(np.arange(self.n_vars), np.diff(self.row_ptr))
-        lower_mask = slot < self.diag_ptr[row]
-        updates = int(upper[self.col_ind[lower_mask]].sum())
-        return multipliers, updates, multipliers + int(upper.sum())
+    def counts(self) -> tuple[int, int, int]:
+        """``(multipliers, updates, substitutions)``: one factorisation's scalings and
+        multiply-adds, and one solve's multiply-adds (both substitutions)."""
+        multipliers = int(self.plan.mult.size)
+        return multipliers, self.plan.n_updates, self.nnz - self.n_vars
 
 
-def analyse(pattern: tuple[tuple[int, ...], ...], ordering: str = "amd") -> SparseLULayout:
-    """Order, factorise symbolically, and lay out ``L + U`` in CSR."""
-    n_vars = len(pattern)
+def _plan_updates(indptr: np.ndarray, indices: np.ndarray, diag: np.ndarray) -> UpdatePlan:
+    n = indptr.size - 1
+    row_begin, mult, pivot, src_begin, src_end, dst_begin, dst = [0], [], [], [], [], [], []
+    for i in range(n):
+        lo, hi = int(indptr[i]), int(indptr[i + 1])
+        where = {int(c): s for s, c in zip(range(lo, hi), indices[lo:hi])}
+        for p in range(lo, int(diag[i])):
+            k = int(indices[p])
+            s0, s1 = int(diag[k]) + 1, int(indptr[k + 1])
+            mult.append(p)
+            pivot.append(int(diag[k]))
+            src_begin.append(s0)
+            src_end.append(s1)
+            dst_begin.append(len(dst))
+            dst.extend(where[int(c)] for c in indices[s0:s1])
+        row_begin.append(len(mult))
+    as32 = lambda v: np.asarray(v, dtype=np.int32)  # noqa: E731
+    return UpdatePlan(as32(row_begin), as32(mult), as32(pivot), as32(src_begin), as32(src_end),
+                      as32(dst_begin), as32(dst))
+
+
+def analyse(pattern: tuple[tuple[int, ...], ...], ordering: str = "amd") -> LUStructure:
+    """Order the pattern, factorise it symbolically and lay ``L + U`` out in CSR."""
     order = fill_reducing_order(pattern, ordering)
-    forward = np.asarray(order, dtype=np.int64)
-    inverse = np.empty(n_vars, dtype=np.int64)
-    inverse[forward] = np.arange(n_vars)
-    filled = fill_pattern(
-        tuple(
-            tuple(sorted(int(inverse[c]) for c in pattern[int(forward[i])]))
-            for i in range(n_vars)
-        )
-    )
-    row_ptr = np.zeros(n_vars + 1, dtype=np.int32)
-    row_ptr[1:] = np.cumsum(filled.sum(axis=1))
-    col_ind = np.concatenate([np.flatnonzero(filled[i]) for i in range(n_vars)]).astype(np.int32)
-    diag_ptr = np.array(
-        [int(row_ptr[i]) + int(np.searchsorted(col_ind[row_ptr[i]:row_ptr[i + 1]], i))
-         for i in range(n_vars)],
-        dtype=np.int32,
-    )
-    return SparseLULayout(n_vars, tuple(int(i) for i in order), row_ptr, col_ind, diag_ptr)
+    position = np.empty(len(order), dtype=np.int64)
+    position[np.asarray(order, dtype=np.int64)] = np.arange(len(order))
+    permuted = [sorted(int(position[c]) for c in pattern[v]) for v in order]
+    rows = symbolic_rows(permuted)
+    indptr = np.concatenate([[0], np.cumsum([r.size for r in rows])]).astype(np.int32)
+    indices = np.concatenate(rows).astype(np.int32) if rows else np.zeros(0, dtype=np.int32)
+    diag = np.array([int(indptr[i]) + int(np.searchsorted(r, i)) for i, r in enumerate(rows)],
+                    dtype=np.int32)
+    return LUStructure(tuple(int(v) for v in order), indptr, indices, diag,
+                       _plan_updates(indptr, indices, diag))
 
 
-def compressed_jacobian(pattern, layout: SparseLULayout) -> CompressedJacobian:
-    """Colour-grid positions remapped onto the factorisation's CSR slots."""
-    compressed = colour_sparsity(pattern)
-    table = layout.slot_table()
-    packed = np.full(layout.n_vars * compressed.n_colours, -1, dtype=np.int64)
-    for row, cols in enumerate(pattern):
-        for col in cols:
-            slot = int(table[row, col])
-            if slot < 0:
-                raise ValueError(
-                    f"entry ({row}, {col}) is in the pattern but not in the "
-                    "factorised structure"
-                )
-            packed[row * compressed.n_colours + compressed.colour[col]] = slot
-    diagonal = np.array([int(table[i, i]) for i in range(layout.n_vars)])
-    return replace(
-        compressed,
-        packed=tuple(int(s) for s in packed),
-        packed_diagonal=tuple(int(s) for s in diagonal),
-        n_slots=layout.nnz,
-    )
+def csr_slot_map(pattern, structure: LUStructure) -> SlotMap:
+    """The pattern's colouring with each sweep value stored at its CSR slot.
+
+    Fill-in slots belong to no Jacobian column and are claimed by no sweep; the
+    kernel clears them before the sweeps."""
+    partition = colour_columns(pattern)
+    table = structure.caller_slots()
+    rows = np.array([r for r, cols in enumerate(pattern) for _ in cols], dtype=np.int64)
+    cols = np.array([c for cs in pattern for c in cs], dtype=np.int64)
+    slots = table[rows, cols]
+    if (slots < 0).any():
+        k = int(np.flatnonzero(slots < 0)[0])
+        raise ValueError(f"entry ({int(rows[k])}, {int(cols[k])}) is in the pattern but not in the "
+                         "factorised structure")
+    writes = np.full((structure.n_vars, partition.n_colours), -1, dtype=np.int64)
+    writes[rows, np.asarray(partition.colour, dtype=np.int64)[cols]] = slots
+    diagonal = tuple(int(s) for s in np.diagonal(table))
+    return SlotMap(partition, writes, diagonal, structure.nnz)
 
 
-class SparseDirectSolver:
-    """A layout plus the Jacobian slot map that fills it; pivots nothing."""
+class SparseLU:
+    """One pattern's structure plus the Jacobian slot map that fills it; pivots nothing."""
 
-    ipiv_size = 1
-
-    def __init__(self, layout: SparseLULayout, compressed: CompressedJacobian):
-        self.layout = layout
-        self.compressed = compressed
-        self.ops = layout.factorization_ops()
+    def __init__(self, structure: LUStructure, slots: SlotMap):
+        self.structure = structure
+        self.slots = slots
 
     @property
     def nnz(self) -> int:
-        return self.layout.nnz
+        return self.structure.nnz
 
     def __repr__(self) -> str:
-        m, u, s = self.layout.flop_counts()
-        return (
-            f"<SparseDirectSolver n_vars={self.layout.n_vars} nnz={self.nnz} "
-            f"factorise={m + u} solve={s} colours={self.compressed.n_colours}>"
-        )
+        m, u, s = self.structure.counts()
+        return (f"SparseLU(n={self.structure.n_vars}, nnz={self.nnz}, colours={self.slots.n_colours}, "
+                f"multipliers={m}, updates={u}, substitutions={s})")
 
 
 @functools.cache
-def sparse_direct_solver_for(pattern, ordering: str = "amd") -> SparseDirectSolver:
-    layout = analyse(pattern, ordering)
-    return SparseDirectSolver(layout, compressed_jacobian(pattern, layout))
+def sparse_lu_for(pattern, ordering: str = "amd") -> SparseLU:
+    """Analysis of a normalised pattern, cached on it."""
+    structure = analyse(pattern, ordering)
+    return SparseLU(structure, csr_slot_map(pattern, structure))
 
 
-def sparse_direct_solver(sparsity, n_vars: int, *, ordering: str = "amd") -> SparseDirectSolver:
-    return sparse_direct_solver_for(normalize_sparsity(sparsity, n_vars), ordering)
+def sparse_lu(sparsity, n_vars: int, *, ordering: str = "amd") -> SparseLU:
+    """Analysis of a pattern in any form ``normalize_sparsity`` accepts."""
+    return sparse_lu_for(normalize_sparsity(sparsity, n_vars), ordering)
 
 
 # --- CUDA emission -------------------------------------------------------------------
@@ -245,8 +281,8 @@ def _c_array(name: str, values) -> str:
     return f"__constant__ int {name}[{max(1, len(values))}] = {{{body}}};"
 
 
-def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = False) -> str:
-    """``mdx_sparse_factorize`` / ``mdx_sparse_solve`` / ``mdx_sparse_solve_t`` for one layout.
+def emit_cuda(structure: LUStructure, mode: str = "auto", fast: bool = False) -> str:
+    """``mdx_sparse_factorize`` / ``mdx_sparse_solve`` / ``mdx_sparse_solve_t`` for one structure.
 
     ``T`` is the LU element type.  Multipliers and updates run in ``T`` and the
     reciprocal pivot is formed in double, as ``modax`` does (numba's typing of
@@ -259,52 +295,53 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
     """
     if mode not in ("auto", "unrolled", "tables"):
         raise ValueError(f"sparse code mode must be 'auto', 'unrolled' or 'tables'; got {mode!r}")
-    n = layout.n_vars
-    row_ptr, diag_ptr = layout.row_ptr, layout.diag_ptr
-    origin, col_origin = layout.row_origin, layout.col_origin
-    dst_start, destination, upper_end = ops
-    pivot_of = diag_ptr[layout.col_ind]
-    _, updates, substitutions = layout.flop_counts()
+    n = structure.n_vars
+    indptr, diag = structure.indptr, structure.diag
+    origin, col_origin = structure.row_origin, structure.col_origin
+    plan = structure.plan
+    _, updates, substitutions = structure.counts()
     out = []
     # The reciprocal pivot: double then rounded, as the reference types it; in the
     # fast path mdx::fast_recip in the LU type (approximate in FP32).
     recip = "mdx::fast_recip(lu[{0}])" if fast else "(T)(1.0 / (double)lu[{0}])"
 
-    unroll_factor = mode == "unrolled" or (mode == "auto" and destination.size <= MAX_UNROLLED_UPDATES)
+    unroll_factor = mode == "unrolled" or (mode == "auto" and updates <= MAX_UNROLLED_UPDATES)
     unroll_solve = mode == "unrolled" or (mode == "auto" and substitutions <= MAX_UNROLLED_SUBSTITUTIONS)
     if unroll_factor:
         lines = []
         for i in range(n):
-            for p in range(int(row_ptr[i]), int(diag_ptr[i])):
-                above = int(pivot_of[p])
+            for j in range(int(plan.row_begin[i]), int(plan.row_begin[i + 1])):
+                p, above = int(plan.mult[j]), int(plan.pivot[j])
                 lines.append(f"  const T f{p} = lu[{p}] * lu[{above}]; lu[{p}] = f{p};")
-                q = int(dst_start[p])
-                for s in range(above + 1, int(upper_end[p])):
-                    lines.append(f"  lu[{int(destination[q])}] -= f{p} * lu[{s}];")
+                q = int(plan.dst_begin[j])
+                for s in range(int(plan.src_begin[j]), int(plan.src_end[j])):
+                    lines.append(f"  lu[{int(plan.dst[q])}] -= f{p} * lu[{s}];")
                     q += 1
-            pivot = int(diag_ptr[i])
+            pivot = int(diag[i])
             lines.append(f"  lu[{pivot}] = {recip.format(pivot)};")
         out.append(
             "template <typename T, class LU> __device__ __forceinline__ void mdx_sparse_factorize(LU& lu) {\n"
             + "\n".join(lines) + "\n}"
         )
     else:
-        out.append(_c_array("mdx_lu_row", row_ptr))
-        out.append(_c_array("mdx_lu_diag", diag_ptr))
-        out.append(_c_array("mdx_lu_pivot", pivot_of))
-        out.append(_c_array("mdx_lu_start", dst_start))
-        out.append(_c_array("mdx_lu_end", upper_end))
-        out.append(_c_array("mdx_lu_dst", destination))
+        out.append(_c_array("mdx_lu_rowj", plan.row_begin))
+        out.append(_c_array("mdx_lu_diag", diag))
+        out.append(_c_array("mdx_lu_mult", plan.mult))
+        out.append(_c_array("mdx_lu_pivot", plan.pivot))
+        out.append(_c_array("mdx_lu_src", plan.src_begin))
+        out.append(_c_array("mdx_lu_srcend", plan.src_end))
+        out.append(_c_array("mdx_lu_dst0", plan.dst_begin))
+        out.append(_c_array("mdx_lu_dst", plan.dst))
         out.append(
             "template <typename T, class LU> __device__ __forceinline__ void mdx_sparse_factorize(LU& lu) {\n"
             f"  for (int i = 0; i < {n}; ++i) {{\n"
-            "    const int pivot = mdx_lu_diag[i];\n"
-            "    for (int p = mdx_lu_row[i]; p < pivot; ++p) {\n"
-            "      const int above = mdx_lu_pivot[p];\n"
-            "      const T f = lu[p] * lu[above]; lu[p] = f;\n"
-            "      int q = mdx_lu_start[p];\n"
-            "      for (int s = above + 1; s < mdx_lu_end[p]; ++s, ++q) lu[mdx_lu_dst[q]] -= f * lu[s];\n"
+            "    for (int j = mdx_lu_rowj[i]; j < mdx_lu_rowj[i + 1]; ++j) {\n"
+            "      const int p = mdx_lu_mult[j];\n"
+            "      const T f = lu[p] * lu[mdx_lu_pivot[j]]; lu[p] = f;\n"
+            "      int q = mdx_lu_dst0[j];\n"
+            "      for (int s = mdx_lu_src[j]; s < mdx_lu_srcend[j]; ++s, ++q) lu[mdx_lu_dst[q]] -= f * lu[s];\n"
             "    }\n"
+            "    const int pivot = mdx_lu_diag[i];\n"
             f"    lu[pivot] = {recip.format('pivot')};\n"
             "  }\n}"
         )
@@ -314,12 +351,12 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
         for i in range(n):
             row = int(origin[i])
             terms = "".join(
-                f" - lu[{p}] * rhs[{int(col_origin[p])}]" for p in range(int(row_ptr[i]), int(diag_ptr[i]))
+                f" - lu[{p}] * rhs[{int(col_origin[p])}]" for p in range(int(indptr[i]), int(diag[i]))
             )
             fwd.append(f"  rhs[{row}] = rhs[{row}]{terms};")
         for i in range(n - 1, -1, -1):
-            row, pivot = int(origin[i]), int(diag_ptr[i])
-            upper = range(pivot + 1, int(row_ptr[i + 1]))
+            row, pivot = int(origin[i]), int(diag[i])
+            upper = range(pivot + 1, int(indptr[i + 1]))
             # The fast path subtracts the back substitution's terms latest-solved
             # last (descending column), so a row waits on one FMA after its last
             # input instead of on all of them; the reference's order is ascending.
@@ -328,13 +365,13 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
         # Transposed: U^T z = b by rows of U in elimination order (scatter),
         # then L^T w = z by rows of L in reverse order (scatter).
         for i in range(n):
-            row, pivot = int(origin[i]), int(diag_ptr[i])
+            row, pivot = int(origin[i]), int(diag[i])
             tfwd.append(f"  rhs[{row}] = rhs[{row}] * lu[{pivot}];")
-            for p in range(pivot + 1, int(row_ptr[i + 1])):
+            for p in range(pivot + 1, int(indptr[i + 1])):
                 tfwd.append(f"  rhs[{int(col_origin[p])}] -= lu[{p}] * rhs[{row}];")
         for i in range(n - 1, -1, -1):
             row = int(origin[i])
-            for p in range(int(row_ptr[i]), int(diag_ptr[i])):
+            for p in range(int(indptr[i]), int(diag[i])):
                 tback.append(f"  rhs[{int(col_origin[p])}] -= lu[{p}] * rhs[{row}];")
         out.append(
             "template <typename T, class LU, class R> __device__ __forceinline__ void mdx_sparse_solve(const LU& lu, R& rhs) {\n"
@@ -345,8 +382,8 @@ def emit_cuda(layout: SparseLULayout, ops, mode: str = "auto", fast: bool = Fals
             + "\n".join(tfwd + tback) + "\n}"
         )
     else:
-        out.append(_c_array("mdx_sv_row", row_ptr))
-        out.append(_c_array("mdx_sv_diag", diag_ptr))
+        out.append(_c_array("mdx_sv_row", indptr))
+        out.append(_c_array("mdx_sv_diag", diag))
         out.append(_c_array("mdx_sv_origin", origin))
         out.append(_c_array("mdx_sv_col", col_origin))
         out.append(

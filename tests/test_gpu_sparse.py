@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from menodax_b200 import rodas5P, systems
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import normalize_sparsity
 
 pytestmark = pytest.mark.gpu
@@ -27,11 +27,11 @@ def test_vdp_ring_sparse_matches_oracle(oracle, horizon):
     mask = cfg["sparsity"]
     hist, stats = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], rtol=1e-6,
                                 atol=1e-8, lu_precision="fp64", sparsity=mask, return_stats=True)
-    solver = sparse_direct_solver_for(normalize_sparsity(mask, 2 * n_osc), "amd")
+    solver = sparse_lu_for(normalize_sparsity(mask, 2 * n_osc), "amd")
     h, a, r, _ = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span,
                               cfg["params"], rtol=1e-6, atol=1e-8, lu_precision="fp64",
-                              sparsity_mask=mask, colour=solver.compressed.colour,
-                              order=solver.layout.order)
+                              sparsity_mask=mask, colour=solver.slots.colour,
+                              order=solver.structure.order)
     same = (np.asarray(stats["accepted_steps"]) == a) & (np.asarray(stats["rejected_steps"]) == r)
     assert same.mean() >= 0.999
     if horizon <= 30.0:

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from menodax_b200 import rodas5P, systems
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import normalize_sparsity
 
 pytestmark = pytest.mark.gpu
@@ -31,8 +31,8 @@ def test_team_vdp_ring_fp64_matches_oracle(oracle, team, layout):
                                 return_stats=True)
     kw = {}
     if mask is not None:
-        solver = sparse_direct_solver_for(normalize_sparsity(mask, 2 * n_osc), "amd")
-        kw = dict(sparsity_mask=mask, colour=solver.compressed.colour, order=solver.layout.order)
+        solver = sparse_lu_for(normalize_sparsity(mask, 2 * n_osc), "amd")
+        kw = dict(sparsity_mask=mask, colour=solver.slots.colour, order=solver.structure.order)
     h, a, r, _ = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span,
                               cfg["params"], rtol=1e-6, atol=1e-8, lu_precision="fp64", **kw)
     same = (np.asarray(stats["accepted_steps"]) == a) & (np.asarray(stats["rejected_steps"]) == r)

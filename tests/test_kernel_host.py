@@ -23,7 +23,7 @@ import pytest
 from menodax_b200 import systems
 from menodax_b200._native import KERNEL_DIR
 from menodax_b200._problem import KernelOptions, build_source
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import normalize_sparsity
 
 PRELUDE = """
@@ -145,8 +145,8 @@ def test_rodas5p_vdp_ring_fp64(tmp_path, oracle, layout):
     hist, counters = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
     kw = {}
     if pattern is not None:
-        solver = sparse_direct_solver_for(pattern, "amd")
-        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.compressed.colour, order=solver.layout.order)
+        solver = sparse_lu_for(pattern, "amd")
+        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.slots.colour, order=solver.structure.order)
     ref = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span, cfg["params"],
                        rtol=1e-6, atol=1e-8, lu_precision="fp64", **kw)
     _agree(hist, counters, ref)

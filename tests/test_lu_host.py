@@ -110,10 +110,10 @@ def test_generated_sparse_lu_solves(tmp_path, mode, t, fast):
     n = 16
     mask = _ring(n)
     layout = analyse(normalize_sparsity(mask, n), "amd")
-    code = emit_cuda(layout, layout.factorization_ops(), mode, fast=fast)
+    code = emit_cuda(layout, mode, fast=fast)
     source = code + f"""
 extern "C" void run(const double* a, const double* b, double* x, int transposed) {{
-  static const int slot[{n * n}] = {{{", ".join(str(int(v)) for v in layout.slot_table().ravel())}}};
+  static const int slot[{n * n}] = {{{", ".join(str(int(v)) for v in layout.caller_slots().ravel())}}};
   {t} lu[{layout.nnz}]; {t} r[{n}];
   for (int i = 0; i < {layout.nnz}; ++i) lu[i] = 0;
   for (int i = 0; i < {n * n}; ++i) if (slot[i] >= 0) lu[slot[i]] = ({t})a[i];

@@ -10,11 +10,11 @@ import pytest
 
 from menodax_b200._sparse_direct import (
     ORDERINGS,
-    SparseDirectSolver,
+    SparseLU,
     analyse,
-    compressed_jacobian,
-    fill_pattern,
-    sparse_direct_solver,
+    csr_slot_map,
+    sparse_lu,
+    symbolic_rows,
 )
 from menodax_b200._sparsity import colour_sparsity, dense_jacobian, normalize_sparsity
 
@@ -60,25 +60,23 @@ def _matrix(mask, seed=0, shift=60.0):
 def _replay(layout, dense):
     """The factorisation and solves the emitted device code performs, in NumPy."""
     n = layout.n_vars
-    row_ptr, col_ind, diag_ptr = layout.row_ptr, layout.col_ind, layout.diag_ptr
-    dst_start, destination, upper_end = layout.factorization_ops()
-    pivot_of = diag_ptr[col_ind]
+    row_ptr, diag_ptr = layout.indptr, layout.diag
+    plan = layout.plan
     origin, col_origin = layout.row_origin, layout.col_origin
     lu = np.zeros(layout.nnz)
-    table = layout.slot_table()
+    table = layout.caller_slots()
     rows, cols = np.nonzero(table >= 0)
     lu[table[rows, cols]] = dense[rows, cols]
     for i in range(n):
-        pivot = diag_ptr[i]
-        for p in range(row_ptr[i], pivot):
-            above = pivot_of[p]
-            f = lu[p] * lu[above]
+        for j in range(plan.row_begin[i], plan.row_begin[i + 1]):
+            p = plan.mult[j]
+            f = lu[p] * lu[plan.pivot[j]]
             lu[p] = f
-            q = dst_start[p]
-            for s in range(above + 1, upper_end[p]):
-                lu[destination[q]] -= f * lu[s]
+            q = plan.dst_begin[j]
+            for s in range(plan.src_begin[j], plan.src_end[j]):
+                lu[plan.dst[q]] -= f * lu[s]
                 q += 1
-        lu[pivot] = 1.0 / lu[pivot]
+        lu[diag_ptr[i]] = 1.0 / lu[diag_ptr[i]]
 
     def solve(b):
         x = np.asarray(b, dtype=np.float64).copy()
@@ -113,11 +111,19 @@ def _replay(layout, dense):
     return solve, solve_t
 
 
-def test_fill_pattern_is_exactly_what_an_unpivoted_lu_touches():
-    mask = _ring(9)
-    predicted = fill_pattern(normalize_sparsity(mask, 9))
-    work = _matrix(mask)
-    for k in range(9):
+@pytest.mark.parametrize("seed", range(6))
+def test_symbolic_rows_are_exactly_what_an_unpivoted_lu_touches(seed):
+    """The up-looking symbolic pass against a numeric right-looking elimination of a
+    random matrix with the same pattern (no cancellation at these values)."""
+    rng = np.random.default_rng(seed)
+    n = 12
+    mask = (rng.random((n, n)) < 0.2) | np.eye(n, dtype=bool)
+    rows = symbolic_rows(normalize_sparsity(mask, n))
+    predicted = np.zeros((n, n), dtype=bool)
+    for i, cols in enumerate(rows):
+        predicted[i, cols] = True
+    work = _matrix(mask, seed=seed)
+    for k in range(n):
         work[k + 1:, k] /= work[k, k]
         work[k + 1:, k + 1:] -= np.outer(work[k + 1:, k], work[k, k + 1:])
     assert ((work != 0.0) == predicted).all()
@@ -160,12 +166,12 @@ MASKS = [_ring(9), _arrow(8), _bordered(4, 2, 5), np.ones((5, 5), dtype=bool)]
 def test_layout_is_a_consistent_csr_image(mask):
     n = len(mask)
     layout = analyse(normalize_sparsity(mask, n), "natural")
-    assert layout.row_ptr[0] == 0 and layout.row_ptr[-1] == layout.nnz
+    assert layout.indptr[0] == 0 and layout.indptr[-1] == layout.nnz
     for i in range(n):
-        span = layout.col_ind[layout.row_ptr[i]:layout.row_ptr[i + 1]]
+        span = layout.indices[layout.indptr[i]:layout.indptr[i + 1]]
         assert (np.diff(span) > 0).all()
-        assert layout.col_ind[layout.diag_ptr[i]] == i
-    table = layout.slot_table()
+        assert layout.indices[layout.diag[i]] == i
+    table = layout.caller_slots()
     slots = [int(table[r, c]) for r, c in zip(*np.nonzero(mask))]
     assert min(slots) >= 0 and len(set(slots)) == len(slots) and max(slots) < layout.nnz
 
@@ -188,16 +194,16 @@ def test_footprint_is_the_factorisation():
     mask = _ring(9)
     pattern = normalize_sparsity(mask, 9)
     layout = analyse(pattern, "natural")
-    compressed = compressed_jacobian(pattern, layout)
+    compressed = csr_slot_map(pattern, layout)
     assert compressed.size == layout.nnz
     assert int((compressed.store_slots() >= 0).sum()) == int(mask.sum()) < compressed.size
     assert len(set(compressed.diagonal)) == 9
 
 
 def test_solver_object_and_cache():
-    a = sparse_direct_solver(_ring(6), 6, ordering="natural")
-    assert isinstance(a, SparseDirectSolver) and a.ipiv_size == 1
-    b = sparse_direct_solver(np.array(sorted(zip(*np.nonzero(_ring(6))))), 6, ordering="natural")
+    a = sparse_lu(_ring(6), 6, ordering="natural")
+    assert isinstance(a, SparseLU) and "nnz=" in repr(a)
+    b = sparse_lu(np.array(sorted(zip(*np.nonzero(_ring(6))))), 6, ordering="natural")
     assert a is b
 
 
@@ -222,11 +228,11 @@ def test_dense_is_row_major():
 
 
 def test_orthogonality_is_checked():
-    from menodax_b200._sparsity import CompressedJacobian, check_orthogonal
+    from menodax_b200._sparsity import assert_orthogonal
 
-    bad = CompressedJacobian(n_vars=2, n_colours=1, colour=(0, 0))
     with pytest.raises(ValueError, match="share colour"):
-        check_orthogonal(((0, 1), (1,)), bad)
+        assert_orthogonal(((0, 1), (1,)), (0, 0))
+    assert_orthogonal(((0, 1), (1,)), (0, 1))
 
 
 def test_seed_table():

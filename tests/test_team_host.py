@@ -16,7 +16,7 @@ import pytest
 
 from menodax_b200 import systems
 from menodax_b200._codegen import emit_neg_jac, emit_rhs
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import dense_jacobian, normalize_sparsity
 from menodax_b200._team import dense_lda, emit_team_functions, group_items, index_expr, slice_bytes
 from menodax_b200._trace import trace
@@ -99,8 +99,8 @@ def test_team_loops_write_what_the_thread_code_writes(tmp_path, name, fn, n, np_
         clear = -0.0
         thread_size = n * n
     else:
-        solver = sparse_direct_solver_for(normalize_sparsity(pattern, n), "amd")
-        structure = solver.compressed
+        solver = sparse_lu_for(normalize_sparsity(pattern, n), "amd")
+        structure = solver.slots
         store = structure.store_slots()
 
         def slot(row, colour):

@@ -23,7 +23,7 @@ import pytest
 from menodax_b200 import systems
 from menodax_b200._native import KERNEL_DIR
 from menodax_b200._problem import KernelOptions, build_source
-from menodax_b200._sparse_direct import sparse_direct_solver_for
+from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import normalize_sparsity
 
 from test_kernel_host import PRELUDE, Args, _host_kernel, _solve
@@ -168,8 +168,8 @@ def test_team_vdp_ring_fp64_matches_oracle(tmp_path, oracle, team, layout):
     hist, counters = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-6, 1e-8)
     kw = {}
     if pattern is not None:
-        solver = sparse_direct_solver_for(pattern, "amd")
-        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.compressed.colour, order=solver.layout.order)
+        solver = sparse_lu_for(pattern, "amd")
+        kw = dict(sparsity_mask=cfg["sparsity"], colour=solver.slots.colour, order=solver.structure.order)
     h, acc, rej, _ = oracle.solve("rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"], t_span,
                                   cfg["params"], rtol=1e-6, atol=1e-8, lu_precision="fp64", **kw)
     _same_steps_and_states(hist, counters, h, acc, rej)

@@ -9,9 +9,10 @@ namespace mdx_internal {
 // in place of the caller's workspace.
 int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* desc, void* stream, int* counter);
 
-// The device of the calling thread's current CUDA context, and whether that
-// context is the device's primary context.
-int current_device(int* device, bool* is_primary);
+// The device of the calling thread's current CUDA context, whether that
+// context is the device's primary context, and (when ctx_id is not NULL) the
+// context's process-unique ID.  Fails when no context is current.
+int current_device(int* device, bool* is_primary, unsigned long long* ctx_id = nullptr);
 
 // Record `message` as the calling thread's last error and return `code`.
 int fail_message(int code, const char* message);

@@ -48,6 +48,10 @@ struct Driver {
   decltype(&cuCtxGetCurrent) ctxGetCurrent = nullptr;
   decltype(&cuCtxSetCurrent) ctxSetCurrent = nullptr;
   decltype(&cuCtxGetDevice) ctxGetDevice = nullptr;
+  decltype(&cuCtxGetId) ctxGetId = nullptr;
+  decltype(&cuCtxPushCurrent) ctxPushCurrent = nullptr;
+  decltype(&cuCtxPopCurrent) ctxPopCurrent = nullptr;
+  decltype(&cuDevicePrimaryCtxGetState) primaryCtxGetState = nullptr;
   decltype(&cuDeviceGet) deviceGet = nullptr;
   decltype(&cuDevicePrimaryCtxRetain) primaryCtxRetain = nullptr;
   decltype(&cuDevicePrimaryCtxRelease) primaryCtxRelease = nullptr;
@@ -90,6 +94,10 @@ void load_driver() {
   resolve("cuCtxGetCurrent", (void**)&g_driver.ctxGetCurrent);
   resolve("cuCtxSetCurrent", (void**)&g_driver.ctxSetCurrent);
   resolve("cuCtxGetDevice", (void**)&g_driver.ctxGetDevice);
+  resolve("cuCtxGetId", (void**)&g_driver.ctxGetId);
+  resolve("cuCtxPushCurrent", (void**)&g_driver.ctxPushCurrent);
+  resolve("cuCtxPopCurrent", (void**)&g_driver.ctxPopCurrent);
+  resolve("cuDevicePrimaryCtxGetState", (void**)&g_driver.primaryCtxGetState);
   resolve("cuDeviceGet", (void**)&g_driver.deviceGet);
   resolve("cuDevicePrimaryCtxRetain", (void**)&g_driver.primaryCtxRetain);
   resolve("cuDevicePrimaryCtxRelease", (void**)&g_driver.primaryCtxRelease);
@@ -123,19 +131,31 @@ int cuda_fail(CUresult r, const char* what) {
 }
 
 // The context launches go to: the calling thread's current one (torch makes the
-// device's primary context current), else device 0's primary context.
+// device's primary context current on first use).  With none current the call
+// is refused rather than a context made current behind the caller's back.
 int current_context(CUcontext* ctx) {
   CUresult r = g_driver.ctxGetCurrent(ctx);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetCurrent");
-  if (*ctx) return MDX_OK;
-  CUdevice dev;
-  if ((r = g_driver.deviceGet(&dev, 0)) != CUDA_SUCCESS) return cuda_fail(r, "cuDeviceGet");
-  if ((r = g_driver.primaryCtxRetain(ctx, dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuDevicePrimaryCtxRetain");
-  if ((r = g_driver.ctxSetCurrent(*ctx)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxSetCurrent");
+  if (!*ctx)
+    return fail(MDX_E_INVALID,
+                "no CUDA context is current on this thread; make the device's context current first "
+                "(cudaSetDevice and any runtime call, or any torch CUDA operation)");
+  return MDX_OK;
+}
+
+// A context's process-unique ID (cuCtxGetId): a context destroyed and created
+// again at the same address gets a new one, so modules cached under the old ID
+// are never launched in the new context.
+int context_id(CUcontext ctx, unsigned long long* id) {
+  CUresult r = g_driver.ctxGetId(ctx, id);
+  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetId");
   return MDX_OK;
 }
 
 struct Loaded {
+  CUcontext ctx = nullptr;
+  CUdevice device = 0;
+  bool primary = false;
   CUmodule module = nullptr;
   CUfunction plain = nullptr;
   CUfunction persistent = nullptr;
@@ -149,31 +169,47 @@ struct mdx_plan {
   mdx_plan_desc desc;
   std::vector<char> cubin;
   std::mutex mu;
-  std::unordered_map<CUcontext, Loaded> loaded;
+  std::unordered_map<unsigned long long, Loaded> loaded;  // by context ID
 };
 
 namespace {
+
+// Unloads a module unless released: every error return after cuModuleLoadData
+// leaves nothing loaded behind.
+struct ModuleGuard {
+  CUmodule module = nullptr;
+  ~ModuleGuard() {
+    if (module) g_driver.moduleUnload(module);
+  }
+};
 
 int load_for_context(mdx_plan* plan, Loaded** out) {
   int rc = require_driver();
   if (rc) return rc;
   CUcontext ctx;
   if ((rc = current_context(&ctx))) return rc;
+  unsigned long long id = 0;
+  if ((rc = context_id(ctx, &id))) return rc;
   std::lock_guard<std::mutex> lock(plan->mu);
-  auto it = plan->loaded.find(ctx);
+  auto it = plan->loaded.find(id);
   if (it != plan->loaded.end()) {
     *out = &it->second;
     return MDX_OK;
   }
   Loaded l;
-  CUresult r = g_driver.moduleLoadData(&l.module, plan->cubin.data());
-  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuModuleLoadData");
-  if ((r = g_driver.moduleGetFunction(&l.plain, l.module, "mdx_solve_plain")) != CUDA_SUCCESS)
+  l.ctx = ctx;
+  ModuleGuard guard;
+  CUresult r = g_driver.moduleLoadData(&guard.module, plan->cubin.data());
+  if (r != CUDA_SUCCESS) {
+    guard.module = nullptr;
+    return cuda_fail(r, "cuModuleLoadData");
+  }
+  if ((r = g_driver.moduleGetFunction(&l.plain, guard.module, "mdx_solve_plain")) != CUDA_SUCCESS)
     return cuda_fail(r, "cuModuleGetFunction(mdx_solve_plain)");
-  if ((r = g_driver.moduleGetFunction(&l.persistent, l.module, "mdx_solve_persistent")) != CUDA_SUCCESS)
+  if ((r = g_driver.moduleGetFunction(&l.persistent, guard.module, "mdx_solve_persistent")) != CUDA_SUCCESS)
     return cuda_fail(r, "cuModuleGetFunction(mdx_solve_persistent)");
   if (plan->desc.flags & MDX_PLAN_ADJOINT) {
-    if ((r = g_driver.moduleGetFunction(&l.grad, l.module, "mdx_grad_reverse")) != CUDA_SUCCESS)
+    if ((r = g_driver.moduleGetFunction(&l.grad, guard.module, "mdx_grad_reverse")) != CUDA_SUCCESS)
       return cuda_fail(r, "cuModuleGetFunction(mdx_grad_reverse)");
   }
   // Above the 48 KB default a kernel's dynamic shared memory has to be opted into.
@@ -183,13 +219,53 @@ int load_for_context(mdx_plan* plan, Loaded** out) {
       if (r != CUDA_SUCCESS) return cuda_fail(r, "cuFuncSetAttribute(MAX_DYNAMIC_SHARED_SIZE_BYTES)");
     }
   }
-  CUdevice dev;
-  if ((r = g_driver.ctxGetDevice(&dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
-  if ((r = g_driver.deviceGetAttribute(&l.sm_count, CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT, dev)) != CUDA_SUCCESS)
+  if ((r = g_driver.ctxGetDevice(&l.device)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
+  if ((r = g_driver.deviceGetAttribute(&l.sm_count, CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT, l.device)) != CUDA_SUCCESS)
     return cuda_fail(r, "cuDeviceGetAttribute");
-  auto res = plan->loaded.emplace(ctx, l);
+  CUcontext primary = nullptr;
+  if ((r = g_driver.primaryCtxRetain(&primary, l.device)) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuDevicePrimaryCtxRetain");
+  g_driver.primaryCtxRelease(l.device);
+  l.primary = primary == ctx;
+  l.module = guard.module;
+  guard.module = nullptr;
+  auto res = plan->loaded.emplace(id, l);
   *out = &res.first->second;
   return MDX_OK;
+}
+
+// Unloads one plan module with its own context current.  A module whose context
+// is gone went with it: a primary context that is inactive, or active under a
+// new ID, is skipped, not pushed.
+int unload_in_context(unsigned long long id, const Loaded& l) {
+  CUcontext ctx = l.ctx;
+  bool release = false;
+  CUresult r;
+  if (l.primary) {
+    unsigned int flags = 0;
+    int active = 0;
+    if ((r = g_driver.primaryCtxGetState(l.device, &flags, &active)) != CUDA_SUCCESS)
+      return cuda_fail(r, "cuDevicePrimaryCtxGetState");
+    if (!active) return MDX_OK;
+    if ((r = g_driver.primaryCtxRetain(&ctx, l.device)) != CUDA_SUCCESS)
+      return cuda_fail(r, "cuDevicePrimaryCtxRetain");
+    release = true;
+    unsigned long long now = 0;
+    if (g_driver.ctxGetId(ctx, &now) != CUDA_SUCCESS || now != id) {
+      g_driver.primaryCtxRelease(l.device);
+      return MDX_OK;
+    }
+  }
+  int rc = MDX_OK;
+  if ((r = g_driver.ctxPushCurrent(ctx)) != CUDA_SUCCESS) {
+    rc = cuda_fail(r, "cuCtxPushCurrent");
+  } else {
+    if ((r = g_driver.moduleUnload(l.module)) != CUDA_SUCCESS) rc = cuda_fail(r, "cuModuleUnload");
+    CUcontext popped;
+    g_driver.ctxPopCurrent(&popped);
+  }
+  if (release) g_driver.primaryCtxRelease(l.device);
+  return rc;
 }
 
 }  // namespace
@@ -283,12 +359,16 @@ int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
 
 int mdx_plan_destroy(mdx_plan* plan) {
   if (!plan) return MDX_OK;
+  int rc = MDX_OK;
   if (g_driver.ok) {
-    for (auto& kv : plan->loaded)
-      if (kv.second.module) g_driver.moduleUnload(kv.second.module);
+    for (auto& kv : plan->loaded) {
+      if (!kv.second.module) continue;
+      const int r = unload_in_context(kv.first, kv.second);
+      if (r && rc == MDX_OK) rc = r;
+    }
   }
   delete plan;
-  return MDX_OK;
+  return rc;
 }
 
 int mdx_workspace_size(const mdx_plan* plan, int mode, int n_traj, size_t* bytes) {
@@ -411,13 +491,13 @@ int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, in
   return MDX_OK;
 }
 
-int current_device(int* device, bool* is_primary) {
+int current_device(int* device, bool* is_primary, unsigned long long* ctx_id) {
   int rc = require_driver();
   if (rc) return rc;
   CUcontext ctx;
-  CUresult r = g_driver.ctxGetCurrent(&ctx);
-  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetCurrent");
-  if (!ctx) return fail(MDX_E_INVALID, "no CUDA context is current on this thread");
+  if ((rc = current_context(&ctx))) return rc;
+  if (ctx_id && (rc = context_id(ctx, ctx_id))) return rc;
+  CUresult r;
   CUdevice dev;
   if ((r = g_driver.ctxGetDevice(&dev)) != CUDA_SUCCESS) return cuda_fail(r, "cuCtxGetDevice");
   CUcontext primary;

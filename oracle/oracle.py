@@ -288,16 +288,37 @@ class System:
         return System(SYS_CALLBACK, n, np_, (), fn)
 
     def _desc(self):
+        """The C descriptor plus what must outlive the call: buffers, the ctypes
+        callbacks and ``errors``, where a Python callback records any exception
+        it raises (ctypes would otherwise print and swallow it, leaving the
+        output undefined); ``_raise_recorded`` turns it into a failed solve."""
         keep = []
         cfg = (ctypes.c_double * max(1, len(self.cfg)))(*self.cfg)
         keep.append(cfg)
         d = _SystemDesc(kind=self.kind, n=self.n, np=self.np, cfg=cfg, n_cfg=len(self.cfg))
+        errors: list[BaseException] = []
+        keep.append(errors)
         if self.kind == SYS_CALLBACK:
             fn = _rebind(self.fn)
             n, np_ = self.n, self.np
 
+            def guarded(body):
+                # IEEE arithmetic as the C side has it: numpy scalars give inf or
+                # nan where Python floats would raise (OverflowError on x ** 2).
+                def run(*args):
+                    out = args[-1]
+                    try:
+                        with np.errstate(all="ignore"):
+                            body(*args)
+                    except BaseException as e:  # noqa: BLE001 -- recorded and re-raised after the solve
+                        errors.append(e)
+                        for i in range(n):
+                            out[i] = math.nan
+                return run
+
             def f_cb(y, t, p, out):
-                vals = fn([y[i] for i in range(n)], t, [p[k] for k in range(np_)])
+                vals = fn([np.float64(y[i]) for i in range(n)], np.float64(t),
+                          [np.float64(p[k]) for k in range(np_)])
                 for i in range(n):
                     out[i] = float(vals[i])
 
@@ -316,10 +337,18 @@ class System:
                     v = Dual.lift(vals[i])
                     out[i] = float(Dual.lift(v.d).d)
 
-            cbs = (F_CB(f_cb), JVP_CB(jvp_cb), JVP2_CB(jvp2_cb))
+            cbs = (F_CB(guarded(f_cb)), JVP_CB(guarded(jvp_cb)), JVP2_CB(guarded(jvp2_cb)))
             keep.extend(cbs)
             d.f_cb, d.jvp_cb, d.jvp2_cb = cbs
         return d, keep
+
+
+def _raise_recorded(keep) -> None:
+    """Fail the oracle call if a Python callback raised during it."""
+    errors = keep[1]
+    if errors:
+        raise RuntimeError(f"the system's Python callback raised {len(errors)} time(s) during the oracle "
+                           f"call; first: {errors[0]!r}") from errors[0]
 
 
 def _ptr(a):
@@ -459,6 +488,7 @@ def solve(solver, system: System, y0, t_span, params, *, rtol=1e-8, atol=1e-10, 
                     diag_ptr=_ptr(arrays.get("diag_ptr")), order=_ptr(arrays.get("order")))
         lib().oracle_rodas5p(ctypes.byref(desc), ctypes.byref(s), ctypes.byref(L), ctypes.byref(ctl),
                              ctypes.byref(ens), 1 if lu_precision == "fp32" else 0, threads)
+    _raise_recorded(keep)
     del keep, cols
     return hist, acc, rej, loop
 
@@ -472,6 +502,7 @@ def jvp(system: System, y, t, p, vy, vt=0.0, vp=None):
     out = np.empty(system.n)
     desc, keep = system._desc()
     lib().oracle_jvp(ctypes.byref(desc), _ptr(y), float(t), _ptr(p), _ptr(vy), float(vt), _ptr(vp), _ptr(out))
+    _raise_recorded(keep)
     del keep
     return out
 
@@ -484,5 +515,6 @@ def jvp2(system: System, y, t, p, uy, ut, up, vy, vt, vp):
     desc, keep = system._desc()
     lib().oracle_jvp2(ctypes.byref(desc), _ptr(y), float(t), _ptr(p), _ptr(uy), float(ut), _ptr(up),
                       _ptr(vy), float(vt), _ptr(vp), _ptr(out))
+    _raise_recorded(keep)
     del keep
     return out

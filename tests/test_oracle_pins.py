@@ -110,6 +110,22 @@ def test_callback_system_matches_builtin(oracle):
     np.testing.assert_allclose(a, b, rtol=1e-10, atol=1e-15)
 
 
+def test_a_raising_callback_fails_the_oracle_call(oracle):
+    """An exception inside a Python callback is recorded and raised after the call,
+    never swallowed with the output left undefined."""
+    calls = [0]
+
+    def broken(y, t, p):
+        calls[0] += 1
+        if calls[0] > 20:
+            raise ZeroDivisionError("planted")
+        return (-p[0] * y[0],)
+
+    with pytest.raises(RuntimeError, match="planted"):
+        oracle.solve("rodas5P", oracle.System.callback(broken, 1, 1), np.ones((2, 1)),
+                     np.linspace(0.0, 1.0, 3), np.ones((2, 1)), lu_precision="fp64", max_steps=50)
+
+
 @pytest.mark.parametrize("solver", ["tsit5", "rodas5P"])
 def test_forward_sensitivities_match_closed_form_cascade(oracle, solver):
     """tests/test_sensitivity.py:42-83, 165-191: jacfwd of the cascade to rtol 1e-6."""

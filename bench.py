@@ -172,7 +172,7 @@ def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    from menodax_b200 import systems
+    from workloads import systems
 
     cfg = systems.robertson_config(size=args.n)
     sample = 8192
@@ -208,7 +208,8 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
     with mu * 1.05.  One step = forward checkpointing solve + reverse sweep."""
     import torch
 
-    from menodax_b200 import rodas5P, systems
+    from menodax_b200 import rodas5P
+    from workloads import systems
 
     cfg = systems.vdp_gradient_config(n_osc, size=n, seed=42 + rank)
     fn = cfg["ode_fn"]
@@ -355,7 +356,8 @@ def run_config(args):
     arithmetic kernel, plus the step statistics and the CPU oracle on a sample."""
     import torch
 
-    from menodax_b200 import _native, autotune, systems
+    from menodax_b200 import _native, autotune
+    from workloads import systems
     from menodax_b200._ensemble import launch
     from menodax_b200._problem import KernelOptions, get_problem
     from menodax_b200._sparsity import normalize_sparsity
@@ -489,7 +491,8 @@ def main():
         return
     import torch
 
-    from menodax_b200 import _native, rodas5P, systems
+    from menodax_b200 import _native, rodas5P
+    from workloads import systems
     from menodax_b200._ensemble import launch
     from menodax_b200._flops import rodas5p_cost
     from menodax_b200._problem import KernelOptions, get_problem

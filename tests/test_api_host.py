@@ -4,7 +4,8 @@ normalisation (modax/_jax_common.py:23-36, modax/rodas5P.py:1204-1211)."""
 import numpy as np
 import pytest
 
-from menodax_b200 import _ensemble, rodas5P, systems, tsit5
+from menodax_b200 import _ensemble, rodas5P, tsit5
+from workloads import systems
 
 
 def test_shape_errors():

@@ -10,7 +10,8 @@ from types import SimpleNamespace
 import pytest
 import torch
 
-from menodax_b200 import _native, autotune, systems
+from menodax_b200 import _native, autotune
+from workloads import systems
 from menodax_b200._problem import KernelOptions
 from menodax_b200._sparsity import normalize_sparsity
 

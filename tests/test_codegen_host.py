@@ -14,7 +14,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from menodax_b200 import systems
+from workloads import systems
 from menodax_b200._codegen import emit_adjoint_pieces, emit_neg_jac, emit_rhs
 from menodax_b200._sparsity import dense_jacobian
 from menodax_b200._trace import TraceError, evaluate, trace

@@ -17,7 +17,8 @@ def _free_port():
 def _worker(rank, world, port, out):
     os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
                       MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    from menodax_b200 import _dist, systems
+    from menodax_b200 import _dist
+    from workloads import systems
 
     r, w, _ = _dist.init(backend="gloo", timeout_s=60)
     cfg = systems.robertson_config(size=8, seed=_dist.shard_seed(42, r))

@@ -14,7 +14,8 @@ rtol 1e-6 within 10 rtol, scaled by |y| + atol/rtol.
 import numpy as np
 import pytest
 
-from menodax_b200 import rodas5P, systems, tsit5
+from menodax_b200 import rodas5P, tsit5
+from workloads import systems
 
 pytestmark = pytest.mark.gpu
 

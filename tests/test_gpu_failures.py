@@ -5,7 +5,8 @@ ends with a status bit, not a hang or a trap."""
 import numpy as np
 import pytest
 
-from menodax_b200 import rodas5P, systems, tsit5
+from menodax_b200 import rodas5P, tsit5
+from workloads import systems
 
 pytestmark = pytest.mark.gpu
 

@@ -4,7 +4,8 @@ import numpy as np
 import pytest
 import torch
 
-from menodax_b200 import rodas5P, systems
+from menodax_b200 import rodas5P
+from workloads import systems
 from menodax_b200.graph import GraphedSolve
 
 pytestmark = pytest.mark.gpu

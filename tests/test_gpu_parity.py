@@ -11,7 +11,8 @@ import numpy as np
 import pytest
 import torch
 
-from menodax_b200 import rodas5P, systems, tsit5
+from menodax_b200 import rodas5P, tsit5
+from workloads import systems
 
 pytestmark = pytest.mark.gpu
 

@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 import torch
 
-from menodax_b200 import rodas5P, sensitivity, systems
+from menodax_b200 import rodas5P, sensitivity
+from workloads import systems
 
 pytestmark = pytest.mark.gpu
 

@@ -12,7 +12,8 @@ import math
 import numpy as np
 import pytest
 
-from menodax_b200 import rodas5P, systems
+from menodax_b200 import rodas5P
+from workloads import systems
 from menodax_b200._sparse_direct import sparse_lu_for
 from menodax_b200._sparsity import normalize_sparsity
 

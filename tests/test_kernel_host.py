@@ -20,7 +20,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from menodax_b200 import systems
+from workloads import systems
 from menodax_b200._native import KERNEL_DIR
 from menodax_b200._problem import KernelOptions, build_source
 from menodax_b200._sparse_direct import sparse_lu_for

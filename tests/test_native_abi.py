@@ -7,7 +7,7 @@ from pathlib import Path
 
 import pytest
 
-from menodax_b200 import systems
+from workloads import systems
 from menodax_b200._problem import KernelOptions, build_source, compile_options
 
 HEADER = Path(__file__).resolve().parents[1] / "include" / "menodax.h"

@@ -8,7 +8,7 @@ before it is trusted as the parity checker.
 import numpy as np
 import pytest
 
-from menodax_b200 import systems
+from workloads import systems
 
 
 def test_lorenz_tsit5_golden_steps(oracle):

@@ -216,7 +216,7 @@ def test_tridiagonal_takes_three_colours():
 
 def test_decay_chain_takes_two_colours():
     """tests/test_sparsity.py:114-116: the chain's four columns in two sweeps."""
-    from menodax_b200 import systems
+    from workloads import systems
 
     compressed = colour_sparsity(normalize_sparsity(systems.DECAY_CHAIN_PATTERN, 4))
     assert compressed.n_colours == 2

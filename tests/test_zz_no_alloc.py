@@ -18,7 +18,8 @@ import numpy as np
 import pytest
 import torch
 
-from menodax_b200 import _native, systems
+from menodax_b200 import _native
+from workloads import systems
 from menodax_b200._problem import KernelOptions, get_problem
 
 pytestmark = pytest.mark.gpu

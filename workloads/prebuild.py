@@ -7,7 +7,8 @@ instead of compiling.  Needs no GPU.
 
 from __future__ import annotations
 
-from menodax_b200 import _native, systems
+from menodax_b200 import _native
+from workloads import systems
 from menodax_b200._problem import KernelOptions, build_source, compile_options
 
 

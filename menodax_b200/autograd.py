@@ -1,7 +1,23 @@
-"""torch.autograd front end: the discrete adjoint of an ensemble solve.
+"""torch.autograd front end: gradients of an ensemble solve.
 
 ``rodas5P.solve`` / ``tsit5.solve`` route here when a torch input requires
-grad.  The forward pass runs the checkpointing kernel, which records every
+grad.  ``sens_error_control`` picks the method, with the reference's meaning
+(``modax/_sensitivity.py:64-135, 331-413``):
+
+* ``True`` (the reference's default): forward sensitivities -- the joint
+  ``[y, S]`` solve with the sensitivities under step-size control, the
+  reference's own differentiation; ``backward`` contracts ``S`` with the
+  incoming cotangent.  The primal output comes from that joint solve, as the
+  reference's does under a JAX transform.
+* ``False``: the discrete adjoint of the plain solve.  Its step sequence is the
+  plain solve's, which is what the reference's forward sensitivities take with
+  error control off, and the gradient equals theirs on that step sequence --
+  computed backwards in one sweep whatever the number of parameters.
+
+``sens_param_columns`` restricts the parameter columns that are differentiated;
+the others receive a zero gradient (the transpose of the reference's gather).
+
+The adjoint's forward pass runs the checkpointing kernel, which records every
 accepted step's size and the start state ``(t, y)`` of every K-th step;
 ``backward`` launches the reverse kernel (``mdx_grad`` in the C ABI), which
 replays each K-step segment from its start state, reverses it step by step and
@@ -148,6 +164,20 @@ class _EnsembleSolve(torch.autograd.Function):
         return grad_y0, grad_p, None, None, None, None, None, None, None
 
 
+class _ColumnMask(torch.autograd.Function):
+    """Identity forward; backward zeroes the gradient of the undifferentiated columns."""
+
+    @staticmethod
+    def forward(ctx, params, keep):
+        ctx.save_for_backward(keep)
+        return params.clone()
+
+    @staticmethod
+    def backward(ctx, grad):
+        (keep,) = ctx.saved_tensors
+        return grad * keep, None
+
+
 class _Problems:
     """The plain problem and its checkpointing/adjoint variants, compiled on demand."""
 
@@ -162,9 +192,85 @@ class _Problems:
         return get_problem(*self.args, opts)
 
 
+class _SensitivitySolve(torch.autograd.Function):
+    """Forward sensitivities: the joint solve forward, ``S^T g`` backward."""
+
+    @staticmethod
+    def forward(ctx, y0, params, run):
+        state, sens, counters = run(y0.detach(), params.detach())
+        ctx.save_for_backward(sens)
+        ctx.n_params = params.shape[1]
+        ctx.wrt_y0 = run.wrt_y0
+        ctx.columns = run.columns
+        ctx.mark_non_differentiable(counters)
+        return state, counters
+
+    @staticmethod
+    def backward(ctx, grad_state, _grad_counters):
+        (sens,) = ctx.saved_tensors
+        n, _, n_vars, _ = sens.shape
+        grad_y0 = grad_p = None
+        offset = 0
+        g = grad_state if grad_state is not None else torch.zeros(sens.shape[:3], dtype=sens.dtype,
+                                                                  device=sens.device)
+        if ctx.wrt_y0:
+            grad_y0 = torch.einsum("nsi,nsij->nj", g, sens[..., :n_vars])
+            offset = n_vars
+        if ctx.columns is not None:
+            grad_p = torch.zeros((n, ctx.n_params), dtype=sens.dtype, device=sens.device)
+            if ctx.columns:
+                grad_p[:, list(ctx.columns)] = torch.einsum("nsi,nsik->nk", g, sens[..., offset:])
+        return grad_y0, grad_p, None
+
+
+class _JointRun:
+    """One joint ``[y, S]`` solve for ``_SensitivitySolve``, fixed but for its inputs."""
+
+    def __init__(self, solver, ode_fn, times, wrt_y0, columns, kw):
+        self.solver, self.ode_fn, self.times, self.kw = solver, ode_fn, times, kw
+        self.wrt_y0 = wrt_y0
+        self.columns = columns  # None: no parameter block; else the differentiated columns
+
+    def __call__(self, y0, params):
+        from menodax_b200 import sensitivity
+
+        state, sens, stats = sensitivity.solve(
+            self.solver, self.ode_fn, y0, self.times, params, wrt_y0=self.wrt_y0,
+            wrt_params=self.columns is not None and len(self.columns) > 0,
+            sens_error_control=True, sens_param_columns=self.columns or None,
+            return_stats=True, **self.kw)
+        counters = torch.stack([stats["accepted_steps"], stats["rejected_steps"], stats["loop_steps"]])
+        return state.contiguous(), sens.contiguous(), counters
+
+
+def _forward_sensitivity_grad(options, ode_fn, y0_t, p_t, times, *, rtol, atol, first_step, max_steps,
+                              return_stats, sens_param_columns):
+    n_params = p_t.shape[1]
+    columns = tuple(range(n_params)) if sens_param_columns is None else tuple(int(c) for c in sens_param_columns)
+    if not p_t.requires_grad:
+        columns = None
+    wrt_y0 = bool(y0_t.requires_grad)
+    if not wrt_y0 and columns is not None and not columns:
+        columns = None
+    if not wrt_y0 and columns is None:
+        raise ValueError("sens_param_columns is empty and y0 does not require grad: nothing to differentiate")
+    kw = dict(rtol=rtol, atol=atol, first_step=first_step, max_steps=max_steps, pcoeff=options.pcoeff,
+              icoeff=options.icoeff, dcoeff=options.dcoeff)
+    if options.solver == "rodas5P":
+        kw.update(lu_precision=options.lu_precision, sparsity=options.sparsity, ordering=options.ordering)
+    run = _JointRun(options.solver, ode_fn, times, wrt_y0, columns, kw)
+    hist, counters = _SensitivitySolve.apply(y0_t, p_t, run)
+    if return_stats:
+        return hist, solver_stats(counters[0], counters[1], counters[2])
+    return hist
+
+
 def solve_with_grad(ode_fn, y0, t_span, params, options, *, rtol, atol, first_step, max_steps,
-                    return_stats, error_weights):
-    """Differentiable ensemble solve; returns torch tensors on the solve's device."""
+                    return_stats, error_weights, sens_error_control=False, sens_param_columns=None):
+    """Differentiable ensemble solve; returns torch tensors on the solve's device.
+
+    ``sens_error_control`` selects forward sensitivities (``True``) or the discrete
+    adjoint (``False``); ``sens_param_columns`` the differentiated parameter columns."""
     if error_weights is not None:
         raise NotImplementedError("error_weights are not supported together with gradients")
     device = pick_device(y0, params)
@@ -184,6 +290,21 @@ def solve_with_grad(ode_fn, y0, t_span, params, options, *, rtol, atol, first_st
         times = t_span.detach().to(device=device, dtype=torch.float64).contiguous()
     else:
         times = torch.as_tensor(t_span, dtype=torch.float64, device=device).contiguous()
+    if sens_param_columns is not None:
+        cols = [int(c) for c in sens_param_columns]
+        if len(set(cols)) != len(cols):
+            raise ValueError("param_columns must not repeat a column")
+        bad = [c for c in cols if not 0 <= c < n_params]
+        if bad:
+            raise ValueError(f"param_columns {bad} lie outside the {n_params} parameter columns")
+    if sens_error_control:
+        return _forward_sensitivity_grad(options, ode_fn, y0_t, p_t, times, rtol=rtol, atol=atol,
+                                         first_step=first_step, max_steps=max_steps,
+                                         return_stats=return_stats, sens_param_columns=sens_param_columns)
+    if sens_param_columns is not None and p_t.requires_grad:
+        keep = torch.zeros(n_params, dtype=torch.float64, device=device)
+        keep[list(int(c) for c in sens_param_columns)] = 1.0
+        p_t = _ColumnMask.apply(p_t, keep)
     problems = _Problems(ode_fn, n_vars, n_params, replace(options, runtime_weights=False))
     key = (ode_fn, n_vars, n_params, options, n, tuple(times.tolist()), float(rtol), float(atol))
     hist, counters = _EnsembleSolve.apply(y0_t, p_t, times, problems, initial_step(first_step), rtol,

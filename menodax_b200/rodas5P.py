@@ -96,6 +96,12 @@ def solve(
     ``autotune.TEAM_MIN_VARS`` or more states.  Teams run the plain system only
     (no save hook, sensitivities or gradients).
 
+    ``array_rhs(y, t, p, out)`` (optional) is the same right-hand side written as
+    an array writer, ``out[i] = ...`` for every component; it is traced like
+    ``ode_fn`` and evaluates the stages, while the Jacobian, ``df/dt`` and every
+    derivative are still taken from ``ode_fn`` (``modax/rodas5P.py:382-391``).
+    The two must compute the same function.
+
     ``save_hook(save_idx, y, t, p_row, acc)`` runs inside the kernel at every save
     (the initial state, each dense-output save, the frozen saves past a
     trajectory's end) on the state at that time; it is traced like ``ode_fn``:
@@ -114,11 +120,8 @@ def solve(
     if arithmetic not in ("auto", "reference", "fast"):
         raise ValueError(f"arithmetic must be 'auto', 'reference' or 'fast'; got {arithmetic!r}")
     fast = arithmetic == "fast" or (arithmetic == "auto" and lu_precision == "fp32")
-    if array_rhs is not None:
-        raise NotImplementedError(
-            "array_rhs is a numba device function; this build traces ode_fn itself "
-            "and needs no separate array form"
-        )
+    if array_rhs is not None and not callable(array_rhs):
+        raise ValueError("array_rhs must be a callable array_rhs(y, t, p, out)")
     if save_hook is not None:
         if hook_size <= 0:
             raise ValueError("a save_hook needs a positive hook_size")
@@ -145,6 +148,7 @@ def solve(
         fast=fast,
         save_hook=save_hook,
         hook_size=int(hook_size) if save_hook is not None else 0,
+        array_rhs=array_rhs,
     )
     from menodax_b200.autograd import needs_grad, solve_with_grad
 
@@ -161,6 +165,7 @@ def solve(
         return solve_with_grad(
             ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
             max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
+            sens_error_control=bool(sens_error_control), sens_param_columns=sens_param_columns,
         )
     return run(
         ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,

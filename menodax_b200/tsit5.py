@@ -76,6 +76,7 @@ def solve(
         return solve_with_grad(
             ode_fn, y0, t_span, params, options, rtol=rtol, atol=atol, first_step=first_step,
             max_steps=max_steps, return_stats=return_stats, error_weights=error_weights,
+            sens_error_control=bool(sens_error_control), sens_param_columns=sens_param_columns,
         )
     return run(
         ode_fn, y0, t_span, params, replace(options, shared_stages=backend == "shared"), rtol=rtol,

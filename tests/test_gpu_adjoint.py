@@ -1,4 +1,6 @@
-"""The discrete adjoint (torch autograd over ``mdx_grad``) against independent gradients.
+"""The discrete adjoint (torch autograd over ``mdx_grad``, ``sens_error_control=False``)
+against independent gradients, and the forward-sensitivity gradient the solvers take
+by default (the reference's method).
 
 * closed-form sensitivities of the linear cascade (tests/test_sensitivity.py:41-83
   in the reference),
@@ -41,7 +43,7 @@ def cascade_exact_sens(t, y0, p):
 def _grads(solve, fn, y0, t_span, params, w, **kw):
     y0_t = torch.tensor(y0, dtype=torch.float64, device="cuda", requires_grad=True)
     p_t = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
-    hist = solve(fn, y0_t, t_span, p_t, **kw)
+    hist = solve(fn, y0_t, t_span, p_t, **{"sens_error_control": False, **kw})
     loss = (hist * torch.as_tensor(w, device="cuda")).sum()
     loss.backward()
     return hist.detach().cpu().numpy(), y0_t.grad.cpu().numpy(), p_t.grad.cpu().numpy()
@@ -229,10 +231,57 @@ def test_fp32_lu_adjoint_agrees_with_fp64_on_a_short_horizon():
     for prec in ("fp64", "fp32"):
         y0_t = y0.clone().requires_grad_(True)
         p_t = mu.clone().requires_grad_(True)
-        h = rodas5P.solve(cfg["ode_fn"], y0_t, t_span, p_t, rtol=1e-6, atol=1e-8, lu_precision=prec)
+        h = rodas5P.solve(cfg["ode_fn"], y0_t, t_span, p_t, rtol=1e-6, atol=1e-8, lu_precision=prec,
+                          sens_error_control=False)
         ((h - target) ** 2).sum().backward()
         grads[prec] = torch.cat([y0_t.grad, p_t.grad], dim=1)
     g64, g32 = grads["fp64"], grads["fp32"]
     rel = (g32 - g64).abs().max(dim=1).values / g64.abs().max(dim=1).values
     assert float(rel.median()) < 1e-4
     assert float(rel.quantile(0.9)) < 1e-3
+
+
+@pytest.mark.parametrize("solve,system,kw", [
+    (rodas5P.solve, "robertson", dict(lu_precision="fp64")),
+    (tsit5.solve, "lorenz", {}),
+])
+def test_default_gradient_is_the_references_forward_sensitivities(oracle, solve, system, kw):
+    """With sens_error_control left at True (the reference's default) the gradient is
+    the forward-sensitivity one with the sensitivities under error control: the
+    oracle's joint solve under error control, contracted with the cotangent."""
+    cfg = getattr(systems, f"{system}_config")(size=32)
+    w = np.random.default_rng(7).normal(size=(32, len(cfg["t_span"]), 3))
+    y0_t = torch.tensor(cfg["y0"], dtype=torch.float64, device="cuda", requires_grad=True)
+    p_t = torch.tensor(cfg["params"], dtype=torch.float64, device="cuda", requires_grad=True)
+    hist = solve(cfg["ode_fn"], y0_t, cfg["t_span"], p_t, rtol=cfg["rtol"], atol=cfg["atol"], **kw)
+    (hist * torch.as_tensor(w, device="cuda")).sum().backward()
+    sys_ = getattr(oracle.System, system)()
+    oh, *_ = oracle.solve("rodas5P" if solve is rodas5P.solve else "tsit5", sys_, cfg["y0"], cfg["t_span"],
+                          cfg["params"], rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64",
+                          sens=(True, list(range(sys_.np)), True))
+    n = sys_.n
+    sens = oh[:, :, n:].reshape(32, len(cfg["t_span"]), n + sys_.np, n)
+    g = np.einsum("nsj,nskj->nk", w, sens)
+    np.testing.assert_allclose(hist.detach().cpu().numpy(), oh[:, :, :n], rtol=1e-9, atol=1e-14)
+    scale = np.abs(g).max(axis=1, keepdims=True)
+    got = np.concatenate([y0_t.grad.cpu().numpy(), p_t.grad.cpu().numpy()], axis=1)
+    assert (np.abs(got - g) / scale).max() < 1e-7
+
+
+@pytest.mark.parametrize("error_control", [True, False])
+def test_sens_param_columns_zero_the_other_columns(error_control):
+    """Only the listed parameter columns are differentiated; the rest get zeros, and
+    the listed ones match the full gradient's."""
+    cfg = systems.robertson_config(size=16)
+    w = np.random.default_rng(8).normal(size=(16, len(cfg["t_span"]), 3))
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64", sens_error_control=error_control)
+
+    def grad(columns):
+        p_t = torch.tensor(cfg["params"], dtype=torch.float64, device="cuda", requires_grad=True)
+        hist = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], p_t, sens_param_columns=columns, **kw)
+        (hist * torch.as_tensor(w, device="cuda")).sum().backward()
+        return p_t.grad.cpu().numpy()
+
+    full, some = grad(None), grad([2, 0])
+    assert (some[:, 1] == 0.0).all()
+    np.testing.assert_allclose(some[:, [0, 2]], full[:, [0, 2]], rtol=1e-9, atol=1e-12 * np.abs(full).max())

@@ -26,7 +26,7 @@ from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
 from menodax_b200._team import TEAM_SIZES, dense_lda, emit_team_functions
 from menodax_b200._team import slice_bytes as team_slice_bytes
 from menodax_b200._sparsity import dense_jacobian
-from menodax_b200._trace import trace, trace_hook
+from menodax_b200._trace import trace, trace_array_rhs, trace_hook
 
 TSIT5_EXPONENT = -1.0 / 5.0   # modax/tsit5.py:90
 DENSE_UNROLL_MAX = 12          # mdx_dense_lu.cuh: register-resident dense LU up to this size
@@ -69,6 +69,9 @@ class KernelOptions:
     # Tsit5: the stage vectors k1..k6 in shared memory, one column per thread
     # (the reference's "shared" backend, modax/tsit5.py:117-139).
     shared_stages: bool = False
+    # Rodas5P: an array-form right-hand side array_rhs(y, t, p, out) for the stage
+    # evaluations; derivatives still come from ode_fn (modax/rodas5P.py:382-391).
+    array_rhs: object = None
 
 
 def controller_exponents(options: KernelOptions):
@@ -126,7 +129,7 @@ def team_block_threads(n_vars: int, n_params: int, options: KernelOptions, prefe
     return threads
 
 
-def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
+def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, stage_tr=None):
     """The team kernel's source: class loops for f, -J and df/dt, the matrix in shared memory."""
     if options.solver != "rodas5P":
         raise ValueError("the team kernel runs Rodas5P")
@@ -146,7 +149,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
         structure = dense_jacobian(n_vars)
         lda = dense_lda(n_vars)
         lu_size = n_vars * lda
-        code = emit_team_functions(tr, structure, lambda row, col: row * lda + col, skip_zero=True)
+        code = emit_team_functions(tr, structure, lambda row, col: row * lda + col, skip_zero=True,
+                                   stage_outputs=stage_tr.outputs if stage_tr is not None else None)
         clear = "-0.0"
         extra.append(f"#define MDX_TEAM_LDA {lda}")
         extra.append("__device__ __forceinline__ int mdx_team_diag_slot(int d) { return d * MDX_TEAM_LDA + d; }")
@@ -162,7 +166,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions):
             slot = int(store[row * structure.n_colours + colour])
             return None if slot < 0 else slot
 
-        code = emit_team_functions(tr, structure, lu_slot, skip_zero=False)
+        code = emit_team_functions(tr, structure, lu_slot, skip_zero=False,
+                                   stage_outputs=stage_tr.outputs if stage_tr is not None else None)
         clear = "0.0"
         diag = ", ".join(str(int(d)) for d in structure.diagonal)
         extra.append(f"__device__ const int mdx_team_diag[{n_vars}] = {{{diag}}};")
@@ -229,10 +234,16 @@ def tsit5_stage_bytes(n_system: int, threads_per_block: int) -> int:
 def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     """Generate the full NVRTC source; returns ``(source, meta)``."""
     tr = trace(ode_fn, n_vars, n_params)
+    # The stage evaluations' right-hand side: array_rhs when given (the plain
+    # solve only, as in the reference: a joint sensitivity system is built from
+    # ode_fn), else ode_fn itself.
+    stage_tr = tr
+    if options.array_rhs is not None and options.sens is None:
+        stage_tr = trace_array_rhs(options.array_rhs, tr)
     if options.shared_stages and options.solver != "tsit5":
         raise ValueError("shared_stages places Tsit5's stage vectors; Rodas5P's shared layout is the team kernel")
     if options.team:
-        return _build_team_source(tr, n_vars, n_params, options)
+        return _build_team_source(tr, n_vars, n_params, options, stage_tr)
     sens = _sens_layout(n_vars, n_params, options.sens)
     n_sens = 0 if sens is None else sens.n_sens
     n_system = n_vars * (1 + n_sens)
@@ -271,7 +282,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         "__device__ __forceinline__ double mdx_const_weight(int j) "
         f"{{ return j < MDX_NV ? 1.0 : {sens_weight}; }}"
     )
-    parts.append(emit_rhs(tr, sens))
+    parts.append(emit_rhs(stage_tr, sens))
     lu_size = 0
     sparse = None
     if rodas:

@@ -154,7 +154,8 @@ class TeamCode:
     n_jac_classes: int
 
 
-def emit_team_functions(tr: TracedRHS, compressed, lu_slot, *, skip_zero: bool) -> TeamCode:
+def emit_team_functions(tr: TracedRHS, compressed, lu_slot, *, skip_zero: bool,
+                        stage_outputs=None) -> TeamCode:
     """The team right-hand side, ``-J`` writer and ``df/dt``.
 
     ``lu_slot(row, colour) -> slot | None`` places the colour-grid entry
@@ -162,12 +163,15 @@ def emit_team_functions(tr: TracedRHS, compressed, lu_slot, *, skip_zero: bool) 
     are the same colour-seeded tangents the thread kernel evaluates, written
     after the caller has cleared the buffer; a structurally zero entry stores
     ``-0.0`` as the thread kernel's does, unless ``skip_zero`` says the clear
-    already wrote ``-0.0`` there (the dense layout)."""
+    already wrote ``-0.0`` there (the dense layout).  ``stage_outputs`` (nodes of
+    the same graph) replace ``tr.outputs`` in the right-hand side only: an
+    array-form right-hand side evaluates the stages, ``tr`` still gives -J."""
     g, n = tr.graph, tr.n_vars
     tables: list[str] = []
     sizes = {"y": n, "p": tr.n_params}
 
-    rhs_classes = group_items(g, [(o, j) for j, o in enumerate(tr.outputs)])
+    rhs_outputs = tr.outputs if stage_outputs is None else stage_outputs
+    rhs_classes = group_items(g, [(o, j) for j, o in enumerate(rhs_outputs)])
     rhs_lines = emit_class_loops(g, rhs_classes, name="r", store=lambda d, v: f"out[{d}] = {v};",
                                  dest_modulus=n, sizes=sizes, tables=tables)
 

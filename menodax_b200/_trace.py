@@ -560,6 +560,63 @@ def trace(ode_fn, n_vars: int, n_params: int) -> TracedRHS:
     )
 
 
+class _OutRow:
+    """``out`` as an array right-hand side sees it: literal-index writes, in order;
+    a read returns the last value written there."""
+
+    def __init__(self, g: Graph, size: int):
+        self._g = g
+        self._size = size
+        self.values: list = [None] * size
+
+    def _index(self, index):
+        try:
+            i = operator.index(index)
+        except TypeError:
+            raise TraceError("out[...] must be indexed with an integer literal") from None
+        if i < 0:
+            i += self._size
+        if not 0 <= i < self._size:
+            raise TraceError(f"out[{index}] is outside its {self._size} entries")
+        return i
+
+    def __setitem__(self, index, value):
+        i = self._index(index)
+        self.values[i] = value.nid if isinstance(value, Sym) else self._g.const(float(value))
+
+    def __getitem__(self, index):
+        i = self._index(index)
+        if self.values[i] is None:
+            raise TraceError(f"out[{i}] is read before the right-hand side writes it")
+        return Sym(self._g, self.values[i])
+
+    def __len__(self):
+        return self._size
+
+
+def trace_array_rhs(array_rhs, primal: TracedRHS) -> TracedRHS:
+    """Trace an array-form right-hand side ``array_rhs(y, t, p, out)`` into the graph
+    of ``primal`` (the same ``y``, ``t`` and ``p`` leaves).
+
+    The result carries ``array_rhs``'s outputs: the kernels evaluate the stages
+    with it while every derivative still comes from ``primal``
+    (``modax/rodas5P.py:382-391``).  Every ``out`` entry must be written."""
+    g = primal.graph
+    out = _OutRow(g, primal.n_vars)
+    fn = _with_shimmed_globals(array_rhs)
+    try:
+        fn(_Vector(g, "y", primal.n_vars), Sym(g, primal.t), _Vector(g, "p", primal.n_params), out)
+    except TraceError:
+        raise
+    except TypeError as exc:
+        raise TraceError(f"tracing array_rhs failed: {exc}") from exc
+    missing = [i for i, v in enumerate(out.values) if v is None]
+    if missing:
+        raise TraceError(f"array_rhs left out{missing} unwritten; it must write all {primal.n_vars} entries")
+    return TracedRHS(graph=g, n_vars=primal.n_vars, n_params=primal.n_params, y=primal.y, t=primal.t,
+                     p=primal.p, outputs=list(out.values))
+
+
 def evaluate(traced: TracedRHS, y, t, p):
     """Evaluate the traced graph in Python floats (host-side check of a trace)."""
     g = traced.graph

@@ -60,3 +60,39 @@ def test_team_option_errors():
         rodas5P.solve(*args, team=8, save_hook=hook, hook_size=1)
     with pytest.raises(ValueError, match="whole warps"):
         rodas5P.solve(*args, team=8, trajectories_per_block=3)
+
+
+def _robertson_array(y, t, p, out):
+    """The Robertson right-hand side written as an array writer."""
+    out[0] = -p[0] * y[0] + p[1] * y[1] * y[2]
+    out[1] = p[0] * y[0] - p[1] * y[1] * y[2] - p[2] * y[1] ** 2
+    out[2] = p[2] * y[1] ** 2
+
+
+def test_array_rhs_traces_into_the_primal_graph():
+    """An array writer of the same expressions lands on the same graph nodes as the
+    tuple form, so the kernels' stage code is the same; derivatives stay with ode_fn."""
+    from menodax_b200._problem import KernelOptions, build_source
+    from menodax_b200._trace import TraceError, trace, trace_array_rhs
+
+    tr = trace(systems.robertson, 3, 3)
+    arr = trace_array_rhs(_robertson_array, tr)
+    assert arr.graph is tr.graph and arr.outputs == tr.outputs
+    plain, _ = build_source(systems.robertson, 3, 3, KernelOptions())
+    with_array, _ = build_source(systems.robertson, 3, 3, KernelOptions(array_rhs=_robertson_array))
+    assert plain == with_array
+
+    def partial(y, t, p, out):
+        out[0] = y[0]
+
+    with pytest.raises(TraceError, match="unwritten"):
+        trace_array_rhs(partial, tr)
+
+    def scaled(y, t, p, out):
+        for i in range(3):
+            out[i] = 2.0 * y[i]
+
+    src, _ = build_source(systems.robertson, 3, 3, KernelOptions(array_rhs=scaled))
+    assert src != plain and "mdx_rhs" in src
+    with pytest.raises(ValueError, match="array_rhs must be a callable"):
+        rodas5P.solve(systems.robertson, np.zeros(3), systems.ROBERTSON_TIMES, np.zeros(3), array_rhs=3)

@@ -202,3 +202,25 @@ def test_tsit5_shared_and_local_backends_agree(which):
     h_shared, s_shared = tsit5.solve(fn, y0, t_span, p, backend="shared", **kw)
     assert np.array_equal(np.asarray(s_local["loop_steps"]), np.asarray(s_shared["loop_steps"]))
     assert np.array_equal(h_local, h_shared)
+
+
+def test_array_rhs_evaluates_the_stages():
+    """modax/rodas5P.py:382-391: an array-form writer of the same right-hand side
+    gives the tuple form's solution (here written with a shared subexpression and
+    in another order, so its stage code differs: FP64 parity bar); the Jacobian
+    still comes from ode_fn."""
+    cfg = systems.robertson_config(size=512)
+
+    def writer(y, t, p, out):
+        fast = p[1] * y[1] * y[2]
+        slow = p[2] * y[1] ** 2
+        out[2] = slow
+        out[0] = fast - p[0] * y[0]
+        out[1] = p[0] * y[0] - fast - slow
+
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64", return_stats=True, launch="plain")
+    h1, s1 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], **kw)
+    h2, s2 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], cfg["params"], array_rhs=writer, **kw)
+    same = (np.asarray(s1["loop_steps"]) == np.asarray(s2["loop_steps"]))
+    assert same.mean() >= 0.999
+    np.testing.assert_allclose(h2[same], h1[same], rtol=1e-9, atol=1e-15)

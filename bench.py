@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_TRAJ)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the compact lines of the other configurations")
     ap.add_argument("--profile", action="store_true",
                     help="only the tuned timed launches (for ncu captures); prints no bench line")
     ap.add_argument("--max-steps", type=int, default=100000,
@@ -199,8 +201,65 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# --------------------------------------------------------------------------- oracle checks
+def error_summary(err, rtol):
+    import numpy as np
+
+    return {"median": float(np.median(err)), "p99": float(np.quantile(err, 0.99)), "max": float(err.max()),
+            "within_10_rtol": float((err <= 10.0 * rtol).mean())}
+
+
+def headline_errors(cfg, outputs, sample):
+    """CPU-baseline leg, used as the checker: each sampled GPU output against the FP64
+    oracle at rtol 1e-12.  A trajectory's error is the largest over its saves and
+    components of |x - x_ref| / (|x_ref| + atol / rtol)."""
+    import numpy as np
+
+    from oracle import oracle
+
+    ref, *_ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"][:sample], cfg["t_span"],
+                           cfg["params"][:sample], rtol=1e-12, atol=1e-14, lu_precision="fp64",
+                           max_steps=10_000_000, threads=oracle.max_threads())
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    out = {name: error_summary((np.abs(h - ref) / scale).reshape(sample, -1).max(axis=1), cfg["rtol"])
+           for name, h in outputs.items()}
+    out["against"] = (f"FP64 oracle at rtol 1e-12, atol 1e-14, first {sample} trajectories; per-trajectory "
+                      "max over saves and components of |x - x_ref| / (|x_ref| + atol/rtol)")
+    return out
+
+
+def gradient_errors(cfg, target, grads, sample):
+    """CPU-baseline leg, used as the checker: each sampled gradient of
+    sum((y - target)^2) against the oracle's forward sensitivities at rtol 1e-10
+    with the sensitivities under error control (the tight gradient).  A
+    trajectory's error is max |g - g_ref| / max |g_ref| over its y0 and mu
+    components."""
+    import numpy as np
+
+    from oracle import oracle
+
+    system = oracle.System.vdp_ring(1, 1.0, 0.1)
+    y0, mu = cfg["y0"][:sample], cfg["params"][:sample]
+    hist, *_ = oracle.solve("rodas5P", system, y0, cfg["t_span"], mu, rtol=1e-10, atol=1e-12,
+                            lu_precision="fp64", sens=(True, [0], True), max_steps=10_000_000,
+                            threads=oracle.max_threads())
+    n = system.n
+    w = 2.0 * (hist[:, :, :n] - target)
+    sens = hist[:, :, n:].reshape(sample, len(cfg["t_span"]), n + 1, n)
+    g_ref = np.einsum("nsj,nskj->nk", w, sens)
+    scale = np.abs(g_ref).max(axis=1)
+    out = {}
+    for name, g in grads.items():
+        rel = np.abs(g - g_ref).max(axis=1) / scale
+        out[name] = {"median": float(np.median(rel)), "p90": float(np.quantile(rel, 0.9)),
+                     "max": float(rel.max()), "within_1e-5": float((rel <= 1e-5).mean())}
+    out["against"] = (f"oracle forward sensitivities at rtol 1e-10 (error control on), first {sample} "
+                      "trajectories, same targets")
+    return out
+
+
 # --------------------------------------------------------------------------- gradients
-def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
+def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=False):
     """Config 5: discrete-adjoint value_and_grad of sum((y - target)^2), device-timed.
 
     VdP (n_osc=1: 2 states), mu ~ log-uniform[10, 500], y0 and mu differentiated,
@@ -227,7 +286,8 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
     def value_and_grad(lu_precision):
         y0_t = y0.clone().requires_grad_(True)
         p_t = mu.clone().requires_grad_(True)
-        hist, stats = rodas5P.solve(fn, y0_t, t, p_t, return_stats=True, **{**kw, "lu_precision": lu_precision})
+        hist, stats = rodas5P.solve(fn, y0_t, t, p_t, return_stats=True, sens_error_control=False,
+                                    **{**kw, "lu_precision": lu_precision})
         loss = ((hist - target) ** 2).sum()
         loss.backward()
         return loss, y0_t.grad, p_t.grad, stats
@@ -309,6 +369,12 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1):
         fms.append((e0, e1))
     barrier(world)
     fs_total = max_over_ranks(sum(a.elapsed_time(b) for a, b in fms), world)
+    if oracle_checks and rank == 0 and world == 1:
+        sample = 256
+        result["error_vs_tight_oracle_gradient"] = gradient_errors(
+            {"y0": cfg["y0"], "params": cfg["params"], "t_span": t}, target[:sample].cpu().numpy(),
+            {"adjoint_fp64": g64[:sample].cpu().numpy(), "adjoint_fp32_lu": g32[:sample].cpu().numpy(),
+             "forward_sensitivities": g_fs[:sample].cpu().numpy()}, sample)
     g_adj = torch.cat([gy, gp], dim=1)
     rel = ((g_adj - g_fs).abs().max(dim=1).values / g_fs.abs().max(dim=1).values.clamp_min(1e-300))
     result["forward_sensitivities"] = {
@@ -350,35 +416,30 @@ def config_roofline(fn, n_vars, n_params, opts, counters, n, n_save, launch_ms, 
             "unit": "TFLOP/s", "frac": t_roof / seconds}
 
 
-def run_config(args):
-    """One line per non-headline configuration: device-timed solves/s of the
-    autotuned FP32-LU kernel (Tsit5: FP64) and of the plain FP64 reference-
-    arithmetic kernel, plus the step statistics and the CPU oracle on a sample."""
+def measure_config(name, steps, warmup, rank, world, *, max_steps=100000, n_limit=None, cpu_baseline=True,
+                   verbose=True, skip=()):
+    """Device-timed solves/s of one non-headline configuration: the autotuned
+    FP32-LU kernel (Tsit5: FP64) and the plain FP64 reference-arithmetic kernel
+    (the reference's design), each with its roofline, plus the step statistics
+    and (rank 0, one GPU) the CPU oracle on a sample.  ``skip`` names variants
+    left out."""
     import torch
 
     from menodax_b200 import _native, autotune
-    from workloads import systems
     from menodax_b200._ensemble import launch
     from menodax_b200._problem import KernelOptions, get_problem
     from menodax_b200._sparsity import normalize_sparsity
+    from workloads import systems
 
-    rank, world, _ = dist_setup(args)
-    if args.config.startswith("grad_"):
-        n_osc = int(args.config[len("grad_vdp"):])
-        n = 65536 if args.n == N_TRAJ else args.n
-        res = measure_gradients(n, args.steps, args.warmup, rank, world, n_osc=n_osc)
-        if rank == 0:
-            print(json.dumps({"config": args.config, **res}))
-        return
     dev = torch.device("cuda", torch.cuda.current_device())
     variants = []
-    if args.config == "lorenz":
+    if name == "lorenz":
         cfg = systems.lorenz_config(size=4096, seed=42 + rank)
         n_vars, n_params = 3, 1
         variants = [("tsit5_fp64", KernelOptions(solver="tsit5"))]
         oracle_sys = ("tsit5", "lorenz", ())
-    elif args.config.startswith("vdp"):
-        n_osc = int(args.config[3:])
+    elif name.startswith("vdp"):
+        n_osc = int(name[3:])
         cfg = systems.vdp_ring_config(n_osc, size=32768, seed=42 + rank)
         n_vars, n_params = 2 * n_osc, 1
         pat = normalize_sparsity(cfg["sparsity"], n_vars)
@@ -400,23 +461,25 @@ def run_config(args):
         pat = normalize_sparsity(cfg["sparsity"], n_vars)
         variants = [("sparse_fp32_fast", KernelOptions(lu_precision="fp32", fast=True, sparsity=pat)),
                     ("dense_fp32", KernelOptions(lu_precision="fp32", fast=True)),
+                    ("plain_fp64_sparse_reference_arith", KernelOptions(lu_precision="fp64", sparsity=pat)),
                     ("plain_fp64_reference_arith", KernelOptions(lu_precision="fp64"))]
         oracle_sys = ("rodas5P", "brusselator", (32,))
-    if args.n != N_TRAJ:
-        cfg = {**cfg, "y0": cfg["y0"][:args.n], "params": cfg["params"][:args.n]}
+    variants = [v for v in variants if v[0] not in skip]
+    if n_limit is not None:
+        cfg = {**cfg, "y0": cfg["y0"][:n_limit], "params": cfg["params"][:n_limit]}
     fn = cfg["ode_fn"]
     n = cfg["y0"].shape[0]
     y0 = torch.as_tensor(cfg["y0"], device=dev).contiguous()
     params = torch.as_tensor(cfg["params"], device=dev).contiguous()
     times = torch.as_tensor(cfg["t_span"], device=dev).contiguous()
     common = dict(y0=y0, times=times, params=params, weights=None, dt0=0.0, rtol=cfg["rtol"],
-                  atol=cfg["atol"], max_steps=args.max_steps)
+                  atol=cfg["atol"], max_steps=max_steps)
     stream = torch.cuda.current_stream(dev)
     results = {}
     stats = None
     peaks = (_native.measure_fma_peak(True), _native.measure_fma_peak(False))
-    for name, opts in variants:
-        if name.startswith("plain"):
+    for vname, opts in variants:
+        if vname.startswith("plain"):
             prob, mode, grid = get_problem(fn, n_vars, n_params, opts), _native.MDX_LAUNCH_PLAIN, 0
             label = "plain, 32 threads/block"
         else:
@@ -434,15 +497,15 @@ def run_config(args):
         # kernel takes 25-36 ms on its first two launches).
         warm_start = time.perf_counter()
         done = 0
-        while done < args.warmup or (time.perf_counter() - warm_start < WARM_S and done < WARM_MAX):
+        while done < warmup or (time.perf_counter() - warm_start < WARM_S and done < WARM_MAX):
             hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
             torch.cuda.synchronize()
             done += 1
         barrier(world)
         ms = []
         # NVTX range per variant: ncu --nvtx --nvtx-include "timed:<variant>/" takes its launches.
-        torch.cuda.nvtx.range_push(f"timed:{name}")
-        for _ in range(args.steps):
+        torch.cuda.nvtx.range_push(f"timed:{vname}")
+        for _ in range(steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -452,32 +515,48 @@ def run_config(args):
         torch.cuda.nvtx.range_pop()
         barrier(world)
         t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ms), world)
-        results[name] = {"solves_per_s": n * world * args.steps / (t * 1e-3), "ms_per_solve": t / args.steps,
-                         "launch": label,
-                         "roofline": config_roofline(fn, n_vars, n_params, opts, counters, n,
-                                                     times.numel(), t / args.steps, peaks)}
-        if rank == 0:
-            print(json.dumps({"config": args.config, "variant": name, **results[name]}), flush=True)
+        loop = counters[2].to(torch.float64)
+        results[vname] = {"solves_per_s": n * world * steps / (t * 1e-3), "ms_per_solve": t / steps,
+                          "launch": label,
+                          "max_steps_fraction": float((counters[3] & 1).to(torch.float64).mean()),
+                          "roofline": config_roofline(fn, n_vars, n_params, opts, counters, n,
+                                                      times.numel(), t / steps, peaks)}
+        if rank == 0 and verbose:
+            print(json.dumps({"config": name, "variant": vname, **results[vname]}), flush=True)
         if stats is None:
-            loop = counters[2].to(torch.float64)
             stats = {"steps_mean": float(loop.mean()), "steps_max": float(loop.max()),
                      "max_steps_hit": int((counters[3] & 1).sum())}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_baseline:
+        # CPU-baseline leg: the oracle timed on a sample of the same ensemble.
         from oracle import oracle
 
         solver, sysname, sysargs = oracle_sys
         system = getattr(oracle.System, sysname)(*sysargs)
-        sample = 256 if n_vars > 8 else 2048
+        sample = min(n, 256 if n_vars > 8 else 2048)
         t0 = time.perf_counter()
         oracle.solve(solver, system, cfg["y0"][:sample], cfg["t_span"], cfg["params"][:sample],
                      rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp32", threads=oracle.max_threads())
         cpu = {"value": sample / (time.perf_counter() - t0), "unit": "solves/s",
                "cores": oracle.max_threads(), "kind": "port", "sample": f"first {sample} trajectories"}
+    return {"config": name, "trajectories": n * world, "n_vars": n_vars, "max_steps": max_steps,
+            "variants": results, "step_stats": stats, "cpu_baseline": cpu}
+
+
+def run_config(args):
+    """``--config``: one line per variant of one configuration, then a summary line."""
+    rank, world, _ = dist_setup(args)
+    if args.config.startswith("grad_"):
+        n_osc = int(args.config[len("grad_vdp"):])
+        n = 65536 if args.n == N_TRAJ else args.n
+        res = measure_gradients(n, args.steps, args.warmup, rank, world, n_osc=n_osc)
+        if rank == 0:
+            print(json.dumps({"config": args.config, **res}))
+        return
+    res = measure_config(args.config, args.steps, args.warmup, rank, world, max_steps=args.max_steps,
+                         n_limit=None if args.n == N_TRAJ else args.n, cpu_baseline=not args.no_cpu_baseline)
     if rank == 0:
-        print(json.dumps({"config": args.config, "trajectories": n * world, "n_vars": n_vars,
-                          "max_steps": args.max_steps, "variants": results, "step_stats": stats,
-                          "cpu_baseline": cpu}))
+        print(json.dumps(res))
 
 
 # --------------------------------------------------------------------------- our arm
@@ -574,6 +653,9 @@ def main():
     value = n * world * args.steps / (total_ms * 1e-3)
     steps_done = counters[2].to(torch.int64).sum().item()
     n_saves = n * (times.numel() - 1)
+    # The timed output's first trajectories, for the error against the oracle.
+    err_sample = min(n, 1024)
+    outputs = {"timed_fp32_lu_fast": hist[:err_sample].cpu().numpy()}
 
     # the plain FP64 one-launch kernel and the other two variants, same ensemble
     variants = {}
@@ -585,6 +667,8 @@ def main():
         v_ms = timed(prob, mode, max(3, args.steps // 2), 2)
         t = max_over_ranks(sum(v_ms), world)
         variants[name] = n * world * len(v_ms) / (t * 1e-3)
+        if name == "plain_fp64_reference_arith":
+            outputs[name] = hist[:err_sample].cpu().numpy()
 
     # roofline of the timed kernel
     cost = rodas5p_cost(fn, 3, 3)
@@ -596,11 +680,15 @@ def main():
     t_roof = per_launch_f64 / peak64 + per_launch_f32 / peak32
     achieved = (per_launch_f64 + per_launch_f32) / launch_s
     blended_peak = (per_launch_f64 + per_launch_f32) / t_roof
+    # DRAM traffic per launch is an ncu figure: it cannot be read inside a timed
+    # run, so it comes from the committed capture of this kernel, labelled as such.
     traffic_path = ROOT / "profiles" / "robertson_traffic.json"
-    traffic = None
+    traffic, traffic_source = None, None
     if traffic_path.exists():
         try:
-            traffic = json.loads(traffic_path.read_text()).get("bytes_per_launch")
+            capture = json.loads(traffic_path.read_text())
+            traffic = capture.get("bytes_per_launch")
+            traffic_source = f"ncu capture in {traffic_path.relative_to(ROOT)} ({capture.get('kernel', '')})"
         except (OSError, ValueError):
             traffic = None
 
@@ -629,14 +717,26 @@ def main():
     h2d = y0_h.numel() * 8 + p_h.numel() * 8 + t_h.numel() * 8
     d2h = out.numel() * 8 + 3 * n * 4
 
-    grads = measure_gradients(n, max(3, args.steps // 2), args.warmup, rank, world)
+    checks = rank == 0 and world == 1 and not args.no_cpu_baseline
+    grads = measure_gradients(n, max(3, args.steps // 2), args.warmup, rank, world, oracle_checks=checks)
+
+    # The other configurations, compactly: every variant device-timed with its
+    # roofline and the fraction of trajectories stopped by max_steps.
+    configs = {}
+    if not args.headline_only:
+        for cname, csteps in (("lorenz", max(3, args.steps // 2)), ("vdp4", 1), ("brusselator", 1)):
+            configs[cname] = measure_config(cname, csteps, 1, rank, world, cpu_baseline=checks, verbose=False)
+        configs["grad_vdp8"] = measure_gradients(n, 1, 1, rank, world, n_osc=8)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    errors = None
+    if checks:
+        # CPU-baseline leg: the oracle timed on a sample, then used as the checker.
         sample = 8192
         rate, threads, _ = cpu_sample_solve(cfg, sample, "fp32")
         cpu = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
                "sample": f"first {sample} of the {n} trajectories, FP32 LU, C++ oracle with OpenMP"}
+        errors = headline_errors(cfg, outputs, err_sample)
 
     if rank == 0:
         line = {
@@ -650,9 +750,14 @@ def main():
             "vs_plain": {k: v for k, v in variants.items()},
             "speedup_vs_plain_fp64": value / variants["plain_fp64_reference_arith"],
             "launch": choice.describe(),
+            "error_vs_oracle": errors,
             "gradients": grads,
+            "configs": configs,
             "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": blended_peak / 1e12,
                          "unit": "TFLOP/s", "frac": achieved / blended_peak, "traffic": traffic,
+                         "traffic_source": traffic_source,
+                         "peak_source": "FP64 / FP32 FMA peaks measured in this run (mdx_measure_fma_peak); "
+                                        "MEASURED_PEAKS.json holds HBM and bf16 tensor figures only",
                          "peak_fp64_measured": peak64 / 1e12, "peak_fp32_measured": peak32 / 1e12,
                          "ops_per_launch_fp64": per_launch_f64, "ops_per_launch_lu_fp32": per_launch_f32,
                          "attempted_steps_per_launch": steps_done},

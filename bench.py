@@ -201,6 +201,23 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def scipy_baseline(cfg, sample):
+    """The reference's own CPU ensemble solver, restated (one scipy ``solve_ivp``
+    per trajectory over a spawn pool of one process per core, LSODA:
+    ``reference/solvers/python/scipy_solve_ivp.py:165-255``), timed on a sample."""
+    from oracle import scipy_ensemble
+    from workloads import systems
+
+    workers = os.cpu_count() or 1
+    rate, _ = scipy_ensemble.timed_rate(systems.robertson, cfg["y0"][:sample], cfg["t_span"],
+                                        cfg["params"][:sample], method="LSODA", rtol=cfg["rtol"],
+                                        atol=cfg["atol"], workers=workers)
+    scipy_ensemble.close()
+    return {"value": rate, "unit": "solves/s", "cores": workers, "kind": "port",
+            "sample": f"first {sample} trajectories, scipy solve_ivp LSODA per trajectory, spawn pool "
+                      "(the reference's scipy_solve_ivp.py approach)"}
+
+
 # --------------------------------------------------------------------------- oracle checks
 def error_summary(err, rtol):
     import numpy as np
@@ -730,6 +747,7 @@ def main():
 
     cpu = None
     errors = None
+    cpu_scipy = None
     if checks:
         # CPU-baseline leg: the oracle timed on a sample, then used as the checker.
         sample = 8192
@@ -737,6 +755,7 @@ def main():
         cpu = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
                "sample": f"first {sample} of the {n} trajectories, FP32 LU, C++ oracle with OpenMP"}
         errors = headline_errors(cfg, outputs, err_sample)
+        cpu_scipy = scipy_baseline(cfg, 2048)
 
     if rank == 0:
         line = {
@@ -762,6 +781,7 @@ def main():
                          "ops_per_launch_fp64": per_launch_f64, "ops_per_launch_lu_fp32": per_launch_f32,
                          "attempted_steps_per_launch": steps_done},
             "cpu_baseline": cpu,
+            "cpu_baseline_scipy": cpu_scipy,
             "clocks": clocks,
             "gpu_launches": args.steps,
         }

@@ -215,3 +215,19 @@ def test_oracle_matches_closed_forms(oracle, solver, name):
     hist, *_ = oracle.solve(solver, oracle.System.callback(fn, n, 1), y, times, params, rtol=1e-10,
                             atol=1e-14, **kw)
     np.testing.assert_allclose(hist, exact(params), rtol=1e-8, atol=1e-10)
+
+
+def test_scipy_ensemble_baseline_solves_the_same_problem(oracle):
+    """The restated scipy_solve_ivp ensemble (the reference's CPU baseline) on a few
+    Robertson trajectories: LSODA at rtol 1e-8 lands near the rtol 1e-12 oracle."""
+    from oracle import scipy_ensemble
+
+    cfg = systems.robertson_config(size=8)
+    try:
+        hist = scipy_ensemble.solve(systems.robertson, cfg["y0"], cfg["t_span"], cfg["params"],
+                                    method="LSODA", rtol=1e-8, atol=1e-12, workers=2)
+    finally:
+        scipy_ensemble.close()
+    ref, *_ = oracle.solve("rodas5P", oracle.System.robertson(), cfg["y0"], cfg["t_span"], cfg["params"],
+                           rtol=1e-12, atol=1e-14, lu_precision="fp64")
+    np.testing.assert_allclose(hist, ref, rtol=1e-5, atol=1e-10)

@@ -91,12 +91,13 @@ class ClockSampler:
         self.uuid = uuid
         self.proc = None
         self.lines = []
+        self.window_start = 0.0
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.uuid}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
@@ -104,7 +105,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark(self):
+        """Keep only the samples taken from now on (the timed region)."""
+        self.window_start = time.monotonic()
 
     def stop(self):
         if self.proc is not None:
@@ -114,7 +119,9 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
         mhz, max_mhz, reasons = [], None, set()
-        for line in self.lines:
+        for stamp, line in self.lines:
+            if stamp < self.window_start:
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -664,8 +671,9 @@ def main():
         torch.cuda.nvtx.range_pop()
         print(json.dumps({"profile": "done", "launch": choice.describe()}))
         return
+    if sampler:
+        sampler.mark()
     ms = timed(tuned, choice.mode, args.steps, args.warmup, tuned_grid)
-    clocks = sampler.stop() if sampler else {}
     total_ms = max_over_ranks(sum(ms), world)
     value = n * world * args.steps / (total_ms * 1e-3)
     steps_done = counters[2].to(torch.int64).sum().item()
@@ -686,6 +694,8 @@ def main():
         variants[name] = n * world * len(v_ms) / (t * 1e-3)
         if name == "plain_fp64_reference_arith":
             outputs[name] = hist[:err_sample].cpu().numpy()
+    # Clock samples cover the timed launches of the headline and its variants.
+    clocks = sampler.stop() if sampler else {}
 
     # roofline of the timed kernel
     cost = rodas5p_cost(fn, 3, 3)

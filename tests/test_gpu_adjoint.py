@@ -271,7 +271,9 @@ def test_default_gradient_is_the_references_forward_sensitivities(oracle, solve,
 @pytest.mark.parametrize("error_control", [True, False])
 def test_sens_param_columns_zero_the_other_columns(error_control):
     """Only the listed parameter columns are differentiated; the rest get zeros, and
-    the listed ones match the full gradient's."""
+    the listed ones match the full gradient's: exactly for the adjoint (the same
+    step sequence), to the solver tolerance under error control, where carrying
+    fewer sensitivity columns changes the error norm and so the steps."""
     cfg = systems.robertson_config(size=16)
     w = np.random.default_rng(8).normal(size=(16, len(cfg["t_span"]), 3))
     kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64", sens_error_control=error_control)
@@ -284,4 +286,5 @@ def test_sens_param_columns_zero_the_other_columns(error_control):
 
     full, some = grad(None), grad([2, 0])
     assert (some[:, 1] == 0.0).all()
-    np.testing.assert_allclose(some[:, [0, 2]], full[:, [0, 2]], rtol=1e-9, atol=1e-12 * np.abs(full).max())
+    tol = 1e-5 if error_control else 1e-9
+    np.testing.assert_allclose(some[:, [0, 2]], full[:, [0, 2]], rtol=tol, atol=tol * 1e-3 * np.abs(full).max())

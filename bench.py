@@ -338,6 +338,9 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
         return total, gy, gp, stats
 
     total, gy, gp, stats = timed("fp64", steps)
+    from menodax_b200 import autograd
+
+    ckpt64 = dict(autograd.last_checkpoint)
     acc = stats["accepted_steps"].to(torch.float64)
     finite = bool(torch.isfinite(gy).all() and torch.isfinite(gp).all())
     # The FP32-LU adjoint (fast arithmetic) on the same ensemble: its own step
@@ -356,6 +359,7 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
                     f"{' sparse LU' if n_osc > 1 else ''}, discrete adjoint, "
                     f"{n} trajectories per GPU, 20 saves on [0, 1000], rtol 1e-6, atol 1e-8",
         "accepted_steps_mean": float(acc.mean()), "accepted_steps_max": float(acc.max()),
+        "checkpoints": ckpt64,
         "gradients_finite": finite,
         "fp32_lu": {
             "value": n * world * fs32 / (total32 * 1e-3), "unit": "gradients/s",

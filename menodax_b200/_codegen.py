@@ -293,7 +293,9 @@ def emit_adjoint_pieces(tr: TracedRHS) -> str:
         "template <class Y, class DB, class YB, class PB>\n"
         "__device__ __forceinline__ void mdx_ft_vjp(const Y& y, const double t, const double* p, const DB& db, YB& yb, PB& pb) {\n"
         + "\n".join(em.lines + lines) + "\n}\n"
+        + "#ifndef MDX_AUTONOMOUS\n"
         + f"#define MDX_AUTONOMOUS {0 if any(x is not None for x in ft) else 1}\n"
+        + "#endif\n"
     )
     return "\n".join(out)
 

@@ -335,6 +335,10 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 f"__device__ __forceinline__ int mdx_diag_slot(int d) {{ switch (d) {{ {cases} default: return 0; }} }}"
             )
         parts.append(emit_neg_jac(tr, structure, lu_size, sens))
+        # df/dt structurally zero (and no sensitivity rows): the stages skip its terms.
+        autonomous = sens is None and all(
+            x is None for x in tr.graph.forward(tr.outputs, {tr.t: tr.graph.const(1.0)}))
+        parts.append(f"#define MDX_AUTONOMOUS {1 if autonomous else 0}")
         if options.save_hook is not None:
             hook = trace_hook(options.save_hook, n_system, n_params, int(options.hook_size))
             parts.append(emit_save_hook(hook))

@@ -42,6 +42,8 @@ from menodax_b200._problem import get_problem
 # Checkpoint capacity (accepted steps per trajectory) and stride last used per
 # problem, so a repeated gradient call sizes its buffer without a counting pass.
 _capacity_hint: dict = {}
+# The checkpoint layout of the most recent gradient forward pass (for reports).
+last_checkpoint: dict = {}
 
 # Steps per recorded start state.  One record per step costs (n + 2) doubles a
 # step; a stride K costs 1 + (n + 1) / K and one forward replay per step in the
@@ -125,6 +127,7 @@ class _EnsembleSolve(torch.autograd.Function):
             capacity = int(needed * 1.1) + 8
             del ckpt
         _capacity_hint[key] = (max(needed + 8, int(needed * 1.1)), stride)
+        last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes)
         ctx.problem = problem
         ctx.capacity = capacity
         ctx.save_for_backward(pc, times, ckpt, ckpt_count)

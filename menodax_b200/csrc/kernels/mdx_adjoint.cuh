@@ -95,12 +95,12 @@ __device__ __forceinline__ void recompute(double t, double h, const double (&y)[
     for (int j = 0; j < MDX_NV; ++j) {
       double value;
       if (s == 0) {
-        value = work[j] + h * coef_d(0) * dT[j];
+        value = MDX_AUTONOMOUS ? work[j] : work[j] + h * coef_d(0) * dT[j];
       } else {
         double acc = coef_c(s, 0) * (double)k[0][j];
 #pragma unroll
         for (int m = 1; m < s; ++m) acc += coef_c(s, m) * (double)k[m][j];
-        if (coef_d(s) != 0.0) value = work[j] + h * coef_d(s) * dT[j] + acc * inv_dt;
+        if (coef_d(s) != 0.0 && !MDX_AUTONOMOUS) value = work[j] + h * coef_d(s) * dT[j] + acc * inv_dt;
         else value = work[j] + acc * inv_dt;
       }
       rhs[j] = (T)value;

@@ -26,6 +26,11 @@ namespace mdx {
 namespace rodas5p {
 
 typedef MDX_LU_T lu_t;
+// A right-hand side with no explicit t dependence has df/dt = 0: its stages
+// skip the h d_s df/dt terms, which are exact zeros added to the stage sums.
+#ifndef MDX_AUTONOMOUS
+#define MDX_AUTONOMOUS 0
+#endif
 // The stage increments are rounded to the LU type when stored (the reference's
 // k_stages, modax/rodas5P.py:724).  Small systems keep the rounded values in
 // double registers, which holds the same numbers without converting on every use.
@@ -113,12 +118,13 @@ __device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& 
   for (int j = 0; j < MDX_NS; ++j) {
     double value;
     if constexpr (S == 0) {
-      value = work[j] + dt_use * coef_d(0) * dT[j];
+      if constexpr (MDX_AUTONOMOUS) value = work[j];
+      else value = work[j] + dt_use * coef_d(0) * dT[j];
     } else {
       double acc = coef_c(S, 0) * (double)k[0][j];
 #pragma unroll
       for (int m = 1; m < S; ++m) acc += coef_c(S, m) * (double)k[m][j];
-      if constexpr (coef_d(S) != 0.0) {
+      if constexpr (coef_d(S) != 0.0 && !MDX_AUTONOMOUS) {
         value = work[j] + dt_use * coef_d(S) * dT[j] + acc * inv_dt;
       } else {
         value = work[j] + acc * inv_dt;

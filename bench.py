@@ -283,7 +283,7 @@ def gradient_errors(cfg, target, grads, sample):
 
 
 # --------------------------------------------------------------------------- gradients
-def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=False):
+def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=False, ring_forward_sens=False):
     """Config 5: discrete-adjoint value_and_grad of sum((y - target)^2), device-timed.
 
     VdP (n_osc=1: 2 states), mu ~ log-uniform[10, 500], y0 and mu differentiated,
@@ -368,9 +368,34 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
             "median_rel_diff_vs_fp64": float(rel32.median()),
         },
     }
+    if n_osc > 1 and not ring_forward_sens:
+        return result
     if n_osc > 1:
-        # The joint [y, S] system of forward sensitivities would carry
-        # 2 n_osc (2 n_osc + 1) + 2 n_osc components; it is timed on the 2-state system.
+        # The reference's method on the same GPU for the ring: the joint [y, S]
+        # system carries 2 n_osc (2 n_osc + 2) components (288 at 16 states; its
+        # kernel takes minutes to compile), so it is timed once on the first
+        # FS_SAMPLE trajectories, and only by --config grad_vdp8.
+        from menodax_b200 import sensitivity
+
+        fs_n = min(n, FS_SAMPLE)
+        sensitivity.solve("rodas5P", fn, y0[:64], t, mu[:64], **kw)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        state, sens = sensitivity.solve("rodas5P", fn, y0[:fs_n], t, mu[:fs_n], **kw)
+        g_fs = torch.einsum("nsj,nsjk->nk", 2.0 * (state - target[:fs_n]), sens)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        fs_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        g_adj = torch.cat([gy, gp], dim=1)[:fs_n]
+        rel = ((g_adj - g_fs).abs().max(dim=1).values / g_fs.abs().max(dim=1).values.clamp_min(1e-300))
+        result["forward_sensitivities"] = {
+            "value": fs_n * world / (fs_ms * 1e-3), "unit": "gradients/s",
+            "method": "joint [y, S] Rodas5P solve, sensitivities under error control (the reference's method), "
+                      f"first {fs_n} trajectories, one launch",
+            "median_rel_diff_vs_adjoint": float(rel.median()),
+        }
         return result
 
     # The reference's method on the same GPU: forward sensitivities (the joint
@@ -414,6 +439,7 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
 
 
 # --------------------------------------------------------------------------- other configurations
+FS_SAMPLE = 4096  # trajectories of the ring's forward-sensitivity timing
 WARM_S = 0.5   # seconds of warm-up launches per configuration variant, at least
 WARM_MAX = 50  # and at most this many launches for it
 
@@ -577,7 +603,7 @@ def run_config(args):
     if args.config.startswith("grad_"):
         n_osc = int(args.config[len("grad_vdp"):])
         n = 65536 if args.n == N_TRAJ else args.n
-        res = measure_gradients(n, args.steps, args.warmup, rank, world, n_osc=n_osc)
+        res = measure_gradients(n, args.steps, args.warmup, rank, world, n_osc=n_osc, ring_forward_sens=True)
         if rank == 0:
             print(json.dumps({"config": args.config, **res}))
         return

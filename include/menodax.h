@@ -119,7 +119,10 @@ typedef struct mdx_grad_desc {
   int struct_size;        /* sizeof(mdx_grad_desc) */
   int n_traj;
   int n_save;
-  int reserved;
+  int count;              /* trajectories this launch reverses: order[0..count) (or
+                             0..count without order); 0 = all n_traj.  Splitting a large
+                             ensemble into several launches bounds the reverse kernel's
+                             resident working set */
   const double* times;
   const double* params;
   const double* ckpt;

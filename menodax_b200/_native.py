@@ -78,7 +78,7 @@ class SolveDesc(ctypes.Structure):
 class GradDesc(ctypes.Structure):
     _fields_ = [
         ("struct_size", ctypes.c_int), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int),
-        ("reserved", ctypes.c_int), ("times", ctypes.c_void_p), ("params", ctypes.c_void_p),
+        ("count", ctypes.c_int), ("times", ctypes.c_void_p), ("params", ctypes.c_void_p),
         ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p),
         ("ckpt_capacity", ctypes.c_longlong), ("grad_hist", ctypes.c_void_p),
         ("grad_y0", ctypes.c_void_p), ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p),

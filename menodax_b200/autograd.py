@@ -96,6 +96,17 @@ def _half_fill(problem, n: int) -> int:
     return autotune.grid_blocks(problem, autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5), n)
 
 
+# Trajectories per reverse launch (None: the whole ensemble in one launch).  The
+# reverse kernel of a larger system keeps its stages and their cotangents in
+# local memory; launching the ensemble in slices, longest trajectories first,
+# bounds how much of that is resident at once.
+REVERSE_CHUNK: int | None = None
+
+
+def reverse_chunk(problem, n: int) -> int:
+    return max(1, min(n, REVERSE_CHUNK or n))
+
+
 class _EnsembleSolve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, y0, params, times, problems, dt0, rtol, atol, max_steps, key):
@@ -160,10 +171,13 @@ class _EnsembleSolve(torch.autograd.Function):
         # for only part of a large ensemble at once, and a long trajectory that
         # started in a later wave would set the makespan.
         order = torch.argsort(ckpt_count, descending=True, stable=True).to(torch.int32)
-        d.order = order.data_ptr()
         stream = torch.cuda.current_stream(params.device).cuda_stream
+        chunk = reverse_chunk(problem, n)
         with torch.cuda.device(params.device):
-            problem.plan.grad(d, stream)
+            for first in range(0, n, chunk):
+                d.order = order.data_ptr() + 4 * first
+                d.count = min(chunk, n - first)
+                problem.plan.grad(d, stream)
         return grad_y0, grad_p, None, None, None, None, None, None, None
 
 

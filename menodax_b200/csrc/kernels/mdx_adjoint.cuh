@@ -366,7 +366,7 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
 mdx_grad_reverse(const MdxGradArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n_traj) return;
+  if (i >= a.n_run) return;
   const int traj = a.order ? a.order[i] : i;
   double p[MDX_NP > 0 ? MDX_NP : 1];
 #pragma unroll

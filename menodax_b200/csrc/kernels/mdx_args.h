@@ -52,9 +52,9 @@ typedef struct MdxGradArgs {
   int* status;             /* may be NULL */
   const int* order;        /* may be NULL: thread i takes trajectory order[i] */
   long long ckpt_capacity;
-  int n_traj;
+  int n_traj;              /* trajectories in the buffers (their stride) */
   int n_save;
-  int pad;
+  int n_run;               /* threads of this launch: order[0..n_run) */
 } MdxGradArgs;
 
 #endif

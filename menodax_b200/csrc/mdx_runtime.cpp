@@ -524,6 +524,8 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
     return fail(MDX_E_INVALID, "mdx_grad_desc.struct_size %d != %d", d->struct_size, (int)sizeof(mdx_grad_desc));
   if (!(plan->desc.flags & MDX_PLAN_ADJOINT)) return fail(MDX_E_INVALID, "the plan was built without the adjoint kernel");
   if (d->n_traj < 0 || d->n_save < 1) return fail(MDX_E_INVALID, "bad sizes n_traj=%d n_save=%d", d->n_traj, d->n_save);
+  if (d->count < 0 || d->count > d->n_traj)
+    return fail(MDX_E_INVALID, "mdx_grad: count %d outside [0, n_traj = %d]", d->count, d->n_traj);
   if (d->n_traj == 0) return MDX_OK;
   if (!d->times || !d->ckpt || !d->ckpt_count || !d->grad_hist || !d->grad_y0 || !d->grad_params ||
       d->ckpt_capacity < 1)
@@ -545,8 +547,9 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
   a.ckpt_capacity = d->ckpt_capacity;
   a.n_traj = d->n_traj;
   a.n_save = d->n_save;
+  a.n_run = d->count > 0 ? d->count : d->n_traj;
   const unsigned tpb = (unsigned)plan->desc.threads_per_block;
-  const unsigned grid = (unsigned)((d->n_traj + tpb - 1) / tpb);
+  const unsigned grid = (unsigned)((a.n_run + tpb - 1) / tpb);
   void* params[] = {&a};
   CUresult r = g_driver.launchKernel(l->grad, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_reverse)");

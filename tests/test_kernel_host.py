@@ -221,7 +221,7 @@ class GradArgs(ctypes.Structure):
                 ("ckpt_count", ctypes.c_void_p), ("grad_hist", ctypes.c_void_p), ("grad_y0", ctypes.c_void_p),
                 ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p), ("order", ctypes.c_void_p),
                 ("ckpt_capacity", ctypes.c_longlong), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int),
-                ("pad", ctypes.c_int)]
+                ("n_run", ctypes.c_int)]
 
 
 def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
@@ -272,7 +272,7 @@ def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity):
         ckpt_count.ctypes.data
     g.grad_hist, g.grad_y0, g.grad_params, g.status = w.ctypes.data, grad_y0.ctypes.data, grad_p.ctypes.data, \
         status.ctypes.data
-    g.ckpt_capacity, g.n_traj, g.n_save = capacity, n, len(times)
+    g.ckpt_capacity, g.n_traj, g.n_save, g.n_run = capacity, n, len(times), n
     lib.run_grad(g)
     assert (status == 0).all()
     return hist, grad_y0, grad_p

@@ -72,3 +72,19 @@ def test_plan_validation(native):
         plan.solve(d, 0)
     assert plan.workspace_size(native.MDX_LAUNCH_PERSISTENT, 100) >= 4
     assert plan.workspace_size(native.MDX_LAUNCH_PLAIN, 100) == 0
+
+
+def test_grad_count_is_validated(native):
+    """mdx_grad's count (trajectories one reverse launch takes) lies in [0, n_traj]."""
+    from menodax_b200._problem import get_problem
+
+    prob = get_problem(systems.cascade, 2, 2, KernelOptions(lu_precision="fp64", checkpoint=True, adjoint=True))
+    d = native.GradDesc()
+    d.n_traj = 4
+    d.n_save = 2
+    d.count = 5
+    with pytest.raises(native.NativeError, match="count 5 outside"):
+        prob.plan.grad(d, 0)
+    d.count = -1
+    with pytest.raises(native.NativeError, match="count -1 outside"):
+        prob.plan.grad(d, 0)

@@ -137,7 +137,8 @@ def emit_class_loops(g: Graph, classes, *, name: str, store, dest_modulus, sizes
         value = em.expr(cls.root) if cls.root is not None else "0.0"
         body = loads + ["  " + ln for ln in em.lines] + [f"    {store(dest, value)}"]
         if n_members == 1:
-            lines.append(f"  if (lane == 0) {{  // class {ci}: 1 member")
+            # Classes of one member go round-robin over the lanes.
+            lines.append(f"  if (lane == {ci} % MDX_TEAM) {{  // class {ci}: 1 member")
             lines.append("    const int m = 0;")
         else:
             lines.append(f"  for (int m = lane; m < {n_members}; m += MDX_TEAM) {{  // class {ci}: {n_members} members")

@@ -23,7 +23,7 @@ from menodax_b200._codegen import (
 )
 from menodax_b200._sparse_direct import MAX_UNROLLED_SUBSTITUTIONS, sparse_lu_for
 from menodax_b200._sparse_direct import emit_cuda as emit_sparse_lu
-from menodax_b200._team import TEAM_SIZES, dense_lda, emit_team_functions
+from menodax_b200._team import TEAM_SIZES, dense_lda, emit_team_adjoint_functions, emit_team_functions
 from menodax_b200._team import slice_bytes as team_slice_bytes
 from menodax_b200._sparsity import dense_jacobian
 from menodax_b200._trace import trace, trace_array_rhs, trace_hook
@@ -135,8 +135,10 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         raise ValueError("the team kernel runs Rodas5P")
     if options.team not in TEAM_SIZES:
         raise ValueError(f"team must be one of {TEAM_SIZES}; got {options.team}")
-    if options.sens is not None or options.save_hook is not None or options.checkpoint or options.adjoint:
-        raise ValueError("the team kernel integrates the plain system: no sens, save_hook, checkpoint or adjoint")
+    if options.sens is not None or options.save_hook is not None:
+        raise ValueError("the team kernel integrates the plain system: no sens or save_hook")
+    if (options.checkpoint or options.adjoint) and options.sparsity is None:
+        raise ValueError("the team kernel's checkpoints and reverse sweep need a sparse LU (a sparsity pattern)")
     tpb = int(options.threads_per_block)
     if tpb % 32 or tpb % options.team:
         raise ValueError(f"threads_per_block {tpb} is not a whole number of warps")
@@ -200,7 +202,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         f"#define MDX_USE_E3 {'true' if e3 != 0.0 else 'false'}",
         f"#define MDX_WEIGHTS_RUNTIME {1 if options.runtime_weights else 0}",
         f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
-        "#define MDX_CHECKPOINT 0",
+        f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
+        f"#define MDX_CKPT_SEG {int(options.ckpt_stride)}",
         "#define MDX_HAS_HOOK 0",
         f"#define MDX_FAST {1 if options.fast else 0}",
         f"#define MDX_TPB {tpb}",
@@ -217,13 +220,51 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         *extra,
         '#include "mdx_team.cuh"',
     ]
+    grad_bytes = 0
+    if options.adjoint:
+        grad_bytes = team_grad_slice_bytes(slice_size, n_vars, n_params, int(options.ckpt_stride),
+                                           autonomous=code.autonomous)
+        if (tpb // options.team) * grad_bytes > STATIC_SHARED_MAX:
+            raise ValueError(
+                f"{tpb // options.team} reverse-sweep slices of {grad_bytes} B exceed a block's static "
+                f"shared memory; use fewer threads per block")
+        parts.append(emit_team_adjoint_functions(tr))
+        parts.append('#include "mdx_team_adjoint.cuh"')
     meta = dict(n_system=n_vars, n_error=n_vars, lu_size=lu_size, sparse=sparse, hook_tables=[],
                 shared_bytes=shared, slice_bytes=slice_size, rhs_classes=code.n_rhs_classes,
-                jac_classes=code.n_jac_classes)
+                jac_classes=code.n_jac_classes, grad_slice_bytes=grad_bytes)
     return "\n".join(parts) + "\n", meta
 
 
 STATIC_SHARED_MAX = 48 * 1024  # a block's static shared memory
+
+
+def team_grad_slice_bytes(slice_bytes: int, n_vars: int, n_params: int, ckpt_stride: int, *,
+                          autonomous: bool) -> int:
+    """Bytes of one trajectory's reverse-sweep slice (``mdx::team_adjoint::GradSlice``):
+    the forward slice, the eight stage cotangents, six (seven with df/dt) vectors,
+    the parameter cotangent and the segment's start states and times."""
+    doubles = 8 * n_vars + (6 if autonomous else 7) * n_vars + max(1, n_params)
+    doubles += ckpt_stride * n_vars + ckpt_stride
+    return slice_bytes + 8 * doubles
+
+
+def team_grad_block_threads(n_vars: int, n_params: int, options: KernelOptions) -> int:
+    """Threads per block of a team gradient module: as many whole-warp teams as let
+    the reverse sweep's slices fit a block's static shared memory (and the forward
+    slices its dynamic shared memory)."""
+    team = int(options.team)
+    sparse = sparse_lu_for(options.sparsity, options.ordering)
+    lu_bytes = 4 if options.lu_precision == "fp32" else 8
+    fwd = team_slice_bytes(n_vars, n_params, sparse.slots.size, lu_bytes, dense=False, autonomous=False,
+                           fast=options.fast)
+    grad = team_grad_slice_bytes(fwd, n_vars, n_params, int(options.ckpt_stride), autonomous=False)
+    teams = max(1, min(STATIC_SHARED_MAX // grad, 128 // team))
+    threads = teams * team // 32 * 32
+    if threads < 32 or (threads // team) * grad > STATIC_SHARED_MAX:
+        raise ValueError(f"a warp of {team}-lane teams needs {32 // team} reverse-sweep slices of {grad} B; "
+                         "they exceed a block's static shared memory")
+    return threads
 
 
 def tsit5_stage_bytes(n_system: int, threads_per_block: int) -> int:

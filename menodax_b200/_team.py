@@ -129,11 +129,9 @@ def emit_class_loops(g: Graph, classes, *, name: str, store, dest_modulus, sizes
             nm = f"{pre}_l{q}"
             loads.append(f"    const double {nm} = {kind}[{ix}];")
             leaf_names[(kind, idx)] = nm
-        em = Emitter(g, {
-            "y": lambda i, _n=leaf_names: _n[("y", i)],
-            "p": lambda i, _n=leaf_names: _n[("p", i)],
-            "t": "t",
-        }, prefix=f"{pre}_v")
+        names = {kind: (lambda i, _k=kind, _n=leaf_names: _n[(_k, i)]) for kind in sizes}
+        names["t"] = "t"
+        em = Emitter(g, names, prefix=f"{pre}_v")
         value = em.expr(cls.root) if cls.root is not None else "0.0"
         body = loads + ["  " + ln for ln in em.lines] + [f"    {store(dest, value)}"]
         if n_members == 1:
@@ -231,3 +229,54 @@ def dense_lda(n_vars: int) -> int:
     """Row stride of the team's dense LU: odd, so a column walk hits 32 banks."""
     return n_vars if n_vars % 2 == 1 else n_vars + 1
 
+
+
+def emit_team_adjoint_functions(tr: TracedRHS) -> str:
+    """Reverse-mode pieces of the team reverse sweep, as class loops.
+
+    The thread kernel's ``mdx_vjp`` / ``mdx_hvp`` / ``mdx_ft_vjp``
+    (``_codegen.emit_adjoint_pieces``), one output component per loop member:
+
+    * ``mdx_team_vjp(y, t, p, r, ub, pb, lane)``: ``ub = J(y)^T r`` (assigned),
+      ``pb += f_p(y)^T r``;
+    * ``mdx_team_hvp(y, t, p, k, r, yb, pb, lane)``: ``(yb, pb) += grad (r . J(y, p) k)``;
+    * ``mdx_team_ft_vjp(y, t, p, d, yb, pb, lane)``: ``(yb, pb) += grad (d . df/dt)``.
+
+    Every output entry is written by exactly one lane, once per call."""
+    g, n, np_ = tr.graph, tr.n_vars, tr.n_params
+    wrt = tr.y + tr.p
+    tables: list[str] = []
+    r = [g.var("r", j) for j in range(n)]
+    sizes = {"y": n, "p": np_, "r": n, "k": n, "d": n}
+
+    def loops(grads, name, assign_state: bool, state_name: str):
+        items_y = [(grads[c], c) for c in range(n)] if assign_state else [
+            (grads[c], c) for c in range(n) if grads[c] is not None]
+        items_p = [(grads[n + k], k) for k in range(np_) if grads[n + k] is not None]
+        op = "=" if assign_state else "+="
+        lines = emit_class_loops(g, group_items(g, items_y), name=f"{name}y",
+                                 store=lambda d, v: f"{state_name}[{d}] {op} {v};", dest_modulus=n,
+                                 sizes=sizes, tables=tables)
+        lines += emit_class_loops(g, group_items(g, items_p), name=f"{name}p",
+                                  store=lambda d, v: f"pb[{d}] += {v};", dest_modulus=None,
+                                  sizes=sizes, tables=tables)
+        return lines
+
+    vjp = loops(g.reverse(tr.outputs, r, wrt), "av", True, "ub")
+    tang = g.forward(tr.outputs, {tr.y[c]: g.var("k", c) for c in range(n)})
+    hvp = loops(g.reverse(tang, r, wrt), "ah", False, "yb")
+    ft = g.forward(tr.outputs, {tr.t: g.const(1.0)})
+    ft_vjp = loops(g.reverse(ft, [g.var("d", j) for j in range(n)], wrt), "af", False, "yb")
+    sig = "const double* __restrict__ y, const double t, const double* __restrict__ p"
+    parts = tables + [
+        f"__device__ __forceinline__ void mdx_team_vjp({sig}, const double* __restrict__ r, "
+        "double* __restrict__ ub, double* __restrict__ pb, const int lane) {",
+        *vjp, "}",
+        f"__device__ __forceinline__ void mdx_team_hvp({sig}, const double* __restrict__ k, "
+        "const double* __restrict__ r, double* __restrict__ yb, double* __restrict__ pb, const int lane) {",
+        *hvp, "}",
+        f"__device__ __forceinline__ void mdx_team_ft_vjp({sig}, const double* __restrict__ d, "
+        "double* __restrict__ yb, double* __restrict__ pb, const int lane) {",
+        *ft_vjp, "}",
+    ]
+    return "\n".join(parts) + "\n"

@@ -93,7 +93,8 @@ def _half_fill(problem, n: int) -> int:
     resident warps each runs with less contention (a 16-state ring's
     checkpointing forward: 0.77 s against 1.21 s for the one-launch kernel;
     unchanged for 2 states)."""
-    return autotune.grid_blocks(problem, autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5), n)
+    choice = autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5, int(problem.options.team))
+    return autotune.grid_blocks(problem, choice, n)
 
 
 # Trajectories per reverse launch (None: the whole ensemble in one launch).  The
@@ -203,9 +204,15 @@ class _Problems:
         self.options = options
 
     def __getitem__(self, which):
-        if which == "plain":
-            return get_problem(*self.args, self.options)
-        opts = replace(self.options, checkpoint=True, adjoint=True, ckpt_stride=int(which))
+        opts = self.options if which == "plain" else replace(
+            self.options, checkpoint=True, adjoint=True, ckpt_stride=int(which))
+        if opts.team:
+            # The reverse sweep's slices take a block's static shared memory.
+            from menodax_b200._problem import team_grad_block_threads
+
+            sized = opts if which != "plain" else replace(opts, ckpt_stride=CKPT_STRIDES[-1])
+            opts = replace(opts, threads_per_block=team_grad_block_threads(
+                self.args[1], self.args[2], replace(sized, checkpoint=True, adjoint=True)))
         return get_problem(*self.args, opts)
 
 

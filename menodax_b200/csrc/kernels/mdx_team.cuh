@@ -96,6 +96,10 @@ __device__ __forceinline__ Slice* slice_of_team() {
 struct State {
   double t, dt, err_prev, err_prev2, tf_local;
   int save_idx, n_steps, accepted, rejected, traj;
+#if MDX_CHECKPOINT
+  int n_ckpt;
+  bool ckpt_overflow;
+#endif
 };
 
 __device__ __forceinline__ size_t hist_index(const MdxSolveArgs& a, int traj, int s, int j) {
@@ -171,6 +175,10 @@ __device__ __forceinline__ void init(State& st, Slice& s, const Lanes& L, const 
   st.tf_local = a.params[(size_t)traj * MDX_NP + MDX_TF_INDEX];
 #else
   st.tf_local = tf;
+#endif
+#if MDX_CHECKPOINT
+  st.n_ckpt = 0;
+  st.ckpt_overflow = false;
 #endif
   __syncwarp(L.mask);
 }
@@ -319,6 +327,21 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
   st.dt = dt_use * factor;
 
   if (accept) {
+#if MDX_CHECKPOINT
+    // The thread kernel's checkpoint layout (mdx_common.cuh::ckpt_write): the
+    // step size, and every MDX_CKPT_SEG-th step's start (t, y), y by component.
+    if (st.n_ckpt < a.ckpt_capacity) {
+      if (L.lane == 0) a.ckpt[(size_t)st.n_ckpt * (size_t)a.n_traj + (size_t)st.traj] = dt_use;
+      if (st.n_ckpt % MDX_CKPT_SEG == 0) {
+        double* rec = ckpt_state(a.ckpt, a.ckpt_capacity, a.n_traj, st.n_ckpt / MDX_CKPT_SEG, st.traj);
+        if (L.lane == 0) rec[0] = t;
+        for (int j = L.lane; j < MDX_NV; j += MDX_TEAM) rec[1 + j] = s.y[j];
+      }
+      ++st.n_ckpt;
+    } else {
+      st.ckpt_overflow = true;
+    }
+#endif
     const double t_new = t + dt_use;
     while (st.save_idx < a.n_save && save_reached(a.times[st.save_idx], t_new)) {
 #if MDX_FAST
@@ -390,7 +413,12 @@ __device__ __forceinline__ void finish(State& st, Slice& s, const Lanes& L, cons
     a.accepted[st.traj] = st.accepted;
     a.rejected[st.traj] = st.rejected;
     a.loop_steps[st.traj] = st.n_steps;
-    if (a.status) a.status[st.traj] = (hit_max ? MDX_STATUS_MAX_STEPS : MDX_STATUS_OK) | (bad ? MDX_STATUS_NONFINITE : 0);
+    int status = (hit_max ? MDX_STATUS_MAX_STEPS : MDX_STATUS_OK) | (bad ? MDX_STATUS_NONFINITE : 0);
+#if MDX_CHECKPOINT
+    if (a.ckpt_count) a.ckpt_count[st.traj] = st.n_ckpt;
+    if (st.ckpt_overflow) status |= MDX_STATUS_CKPT_OVERFLOW;
+#endif
+    if (a.status) a.status[st.traj] = status;
   }
   __syncwarp(L.mask);
 }

@@ -344,8 +344,8 @@ int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
   const int team = desc->team_size;
   if (team != 1 && team != 4 && team != 8 && team != 16 && team != 32)
     return fail(MDX_E_INVALID, "team_size must be 1, 4, 8, 16 or 32; got %d", team);
-  if (team > 1 && (desc->flags & (MDX_PLAN_CHECKPOINT | MDX_PLAN_ADJOINT | MDX_PLAN_SAVE_HOOK)))
-    return fail(MDX_E_INVALID, "a team module (team_size %d) has no checkpoint, adjoint or save-hook kernels", team);
+  if (team > 1 && (desc->flags & MDX_PLAN_SAVE_HOOK))
+    return fail(MDX_E_INVALID, "a team module (team_size %d) has no save-hook kernels", team);
   if (desc->shared_bytes < 0 || desc->shared_bytes > MDX_MAX_SHARED_BYTES)
     return fail(MDX_E_INVALID, "shared_bytes must be in [0, %d]; got %d", MDX_MAX_SHARED_BYTES, desc->shared_bytes);
   mdx_plan* p = new (std::nothrow) mdx_plan;
@@ -549,7 +549,9 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
   a.n_save = d->n_save;
   a.n_run = d->count > 0 ? d->count : d->n_traj;
   const unsigned tpb = (unsigned)plan->desc.threads_per_block;
-  const unsigned grid = (unsigned)((a.n_run + tpb - 1) / tpb);
+  // Trajectories per block: one per thread, or one per team of team_size lanes.
+  const unsigned per_block = tpb / (unsigned)plan->desc.team_size;
+  const unsigned grid = (unsigned)((a.n_run + per_block - 1) / per_block);
   void* params[] = {&a};
   CUresult r = g_driver.launchKernel(l->grad, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
   if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_reverse)");

@@ -93,8 +93,10 @@ def solve(
     ``16`` or ``32`` give each trajectory a team of that many lanes with its
     vectors and matrix in shared memory; ``"auto"`` leaves the choice to the
     launch autotuner, which considers teams for systems of
-    ``autotune.TEAM_MIN_VARS`` or more states.  Teams run the plain system only
-    (no save hook, sensitivities or gradients).
+    ``autotune.TEAM_MIN_VARS`` or more states.  Teams run no save hook and no
+    forward sensitivities; with a sparsity pattern and
+    ``sens_error_control=False`` a team also runs the discrete adjoint (its
+    checkpointing forward pass and its reverse sweep).
 
     ``array_rhs(y, t, p, out)`` (optional) is the same right-hand side written as
     an array writer, ``out[i] = ...`` for every component; it is traced like
@@ -154,11 +156,15 @@ def solve(
 
     grad = needs_grad(y0, params)
     if team_choice:
-        if save_hook is not None or grad:
-            raise ValueError("a team kernel solves the plain system: no save_hook and no gradients")
+        if save_hook is not None:
+            raise ValueError("a team kernel solves the plain system: no save_hook")
+        if grad and (sparsity is None or sens_error_control):
+            raise ValueError("team gradients run the discrete adjoint over a sparse LU: pass a sparsity "
+                             "pattern and sens_error_control=False")
         options = replace(options, team=team_choice)
-        options = replace(options, threads_per_block=team_block_size(
-            team_choice, trajectories_per_block, n_vars, _n_params(params), options))
+        if not grad:
+            options = replace(options, threads_per_block=team_block_size(
+                team_choice, trajectories_per_block, n_vars, _n_params(params), options))
     if grad:
         if save_hook is not None:
             raise NotImplementedError("a solve with a save_hook is not differentiable")

@@ -288,3 +288,21 @@ def test_sens_param_columns_zero_the_other_columns(error_control):
     assert (some[:, 1] == 0.0).all()
     tol = 1e-5 if error_control else 1e-9
     np.testing.assert_allclose(some[:, [0, 2]], full[:, [0, 2]], rtol=tol, atol=tol * 1e-3 * np.abs(full).max())
+
+
+@pytest.mark.parametrize("n_osc", [3, 8])
+def test_team_adjoint_matches_the_thread_adjoint(n_osc):
+    """The team kernels' checkpointing forward pass and reverse sweep (a team of 8
+    lanes per trajectory, its vectors in shared memory) give the thread kernels'
+    gradient on the VdP ring with its sparse LU: the same step sequence and
+    arithmetic, so to rounding."""
+    cfg = systems.vdp_gradient_config(n_osc, size=64)
+    t_span = np.linspace(0.0, 20.0, 6)
+    w = np.random.default_rng(10).normal(size=(64, len(t_span), 2 * n_osc))
+    kw = dict(rtol=1e-6, atol=1e-8, lu_precision="fp64", sparsity=systems.vdp_sparsity(n_osc))
+    h0, gy0, gp0 = _grads(rodas5P.solve, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], w, team=0, **kw)
+    h8, gy8, gp8 = _grads(rodas5P.solve, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], w, team=8, **kw)
+    np.testing.assert_allclose(h8, h0, rtol=1e-9, atol=1e-12)
+    for got, ref in ((gy8, gy0), (gp8, gp0)):
+        scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
+        assert (np.abs(got - ref) / scale).max() < 1e-7

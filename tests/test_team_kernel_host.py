@@ -210,3 +210,118 @@ def test_team_brusselator_dense_fp32_as_accurate_as_fp64(tmp_path, oracle, team)
     err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
     assert np.median(err32) <= 1.5 * np.median(err64) + 10 * cfg["rtol"]
     assert err32.max() <= 3.0 * err64.max()
+
+
+# --- the team reverse sweep ----------------------------------------------------------
+GRAD_DRIVER = """
+static MdxGradArgs host_gargs;
+static void host_grad_lane_main() {
+  mdx_grad_reverse(host_gargs);
+  host_lanes[host_lane].done = true;
+}
+
+extern "C" int run_grad(MdxGradArgs g) {
+  static char stacks[MDX_TPB][1 << 18];
+  host_gargs = g;
+  host_team_size = MDX_TEAM;
+  blockDim.x = MDX_TPB;
+  const int per_block = MDX_TPB / MDX_TEAM;
+  const int blocks = (g.n_run + per_block - 1) / per_block;
+  for (int b = 0; b < blocks; ++b) {
+    blockIdx.x = (unsigned)b;
+    for (int l = 0; l < MDX_TPB; ++l) {
+      HostLane& h = host_lanes[l];
+      h.done = h.waiting = false;
+      getcontext(&h.ctx);
+      h.ctx.uc_stack.ss_sp = stacks[l];
+      h.ctx.uc_stack.ss_size = sizeof(stacks[l]);
+      h.ctx.uc_link = &host_scheduler;
+      makecontext(&h.ctx, host_grad_lane_main, 0);
+    }
+    for (;;) {
+      bool live = false;
+      for (int l = 0; l < MDX_TPB; ++l) {
+        if (host_lanes[l].done || host_lanes[l].waiting) continue;
+        host_lane = (unsigned)l;
+        threadIdx.x = (unsigned)l;
+        swapcontext(&host_scheduler, &host_lanes[l].ctx);
+      }
+      for (int t = 0; t < MDX_TPB / MDX_TEAM; ++t) {
+        int waiting = 0, done = 0;
+        for (int l = t * MDX_TEAM; l < (t + 1) * MDX_TEAM; ++l) {
+          waiting += host_lanes[l].waiting;
+          done += host_lanes[l].done;
+        }
+        if (waiting && done) return 1;
+        if (waiting == MDX_TEAM)
+          for (int l = t * MDX_TEAM; l < (t + 1) * MDX_TEAM; ++l) host_lanes[l].waiting = false;
+        live = live || done < MDX_TEAM;
+      }
+      if (!live) break;
+    }
+  }
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("stride,lu_precision", [(1, "fp64"), (8, "fp64"), (8, "fp32")])
+def test_team_adjoint_matches_oracle_forward_sensitivities(tmp_path, oracle, stride, lu_precision):
+    """The team kernel's checkpointing forward pass and its reverse sweep (class-loop
+    VJPs and Hessian-vector products, the first lane's transposed sparse solves,
+    segment replay) on the VdP ring, against the oracle's forward sensitivities on
+    the same step sequence (1e-7 of the largest component); with FP32 LUs the
+    reverse sweep differentiates the FP32 solve, so it is held against the FP64
+    team gradient at the FP32 LU's accuracy."""
+    from dataclasses import replace
+
+    from oracle.oracle import FMA
+    from menodax_b200._problem import team_grad_block_threads
+    from test_kernel_host import GradArgs, _oracle_sens_grads, _value_and_grad
+
+    n_osc = 3
+    cfg = systems.vdp_gradient_config(n_osc, size=16)
+    t_span = np.linspace(0.0, 5.0, 6)
+    pattern = normalize_sparsity(cfg["sparsity"] if "sparsity" in cfg else systems.vdp_sparsity(n_osc), 2 * n_osc)
+
+    def build(prec):
+        opts = KernelOptions(lu_precision=prec, fast=prec == "fp32", sparsity=pattern, team=8, checkpoint=True,
+                             adjoint=True, ckpt_stride=stride)
+        # One warp per block: the host harness emulates 32 lanes.
+        opts = replace(opts, threads_per_block=min(32, team_grad_block_threads(2 * n_osc, 1, opts)))
+        source, _ = build_source(cfg["ode_fn"], 2 * n_osc, 1, opts)
+        name = f"team_adj_{stride}_{prec}"
+        cpp = tmp_path / f"{name}.cpp"
+        so = tmp_path / f"{name}.so"
+        cpp.write_text(PRELUDE + LANES + "#define MDX_BLOCK_SHARED static\n" + source + DRIVER + GRAD_DRIVER)
+        flags = ["-mfma", "-ffp-contract=fast"] if FMA else ["-ffp-contract=off"]
+        subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-w", *flags, f"-I{KERNEL_DIR}",
+                        str(cpp), "-o", str(so)], check=True)
+        lib = ctypes.CDLL(str(so))
+        lib.run.argtypes = [Args]
+        lib.run.restype = ctypes.c_int
+        lib.run_grad.argtypes = [GradArgs]
+        lib.run_grad.restype = ctypes.c_int
+        return lib
+
+    w = np.random.default_rng(9).normal(size=(16, len(t_span), 2 * n_osc))
+    kw = dict(rtol=1e-8, atol=1e-10)
+    h64, gy64, gp64 = _value_and_grad(build("fp64"), cfg["y0"], t_span, cfg["params"], w, stride=stride,
+                                      capacity=4096, **kw)
+    if lu_precision == "fp64":
+        oh, oy, op = _oracle_sens_grads(oracle, "rodas5P", oracle.System.vdp_ring(n_osc, 1.0, 0.1), cfg["y0"],
+                                        t_span, cfg["params"], w, lu_precision="fp64",
+                                        sparsity_mask=np.asarray(systems.vdp_sparsity(n_osc), dtype=bool),
+                                        colour=sparse_lu_for(pattern, "amd").slots.colour,
+                                        order=sparse_lu_for(pattern, "amd").structure.order, **kw)
+        np.testing.assert_allclose(h64, oh, rtol=1e-9, atol=1e-12)
+        for got, ref in ((gy64, oy), (gp64, op)):
+            scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
+            assert (np.abs(got - ref) / scale).max() < 1e-7
+    else:
+        h32, gy32, gp32 = _value_and_grad(build("fp32"), cfg["y0"], t_span, cfg["params"], w, stride=stride,
+                                          capacity=4096, **kw)
+        g64 = np.concatenate([gy64, gp64], axis=1)
+        g32 = np.concatenate([gy32, gp32], axis=1)
+        rel = np.abs(g32 - g64).max(axis=1) / np.abs(g64).max(axis=1)
+        assert np.median(rel) < 1e-4

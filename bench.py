@@ -310,20 +310,20 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
     with torch.no_grad():
         target = rodas5P.solve(fn, y0, t, mu * 1.05, **kw)
 
-    def value_and_grad(lu_precision):
+    def value_and_grad(lu_precision, **tighter):
         y0_t = y0.clone().requires_grad_(True)
         p_t = mu.clone().requires_grad_(True)
         hist, stats = rodas5P.solve(fn, y0_t, t, p_t, return_stats=True, sens_error_control=False,
-                                    **{**kw, "lu_precision": lu_precision})
+                                    **{**kw, "lu_precision": lu_precision, **tighter})
         loss = ((hist - target) ** 2).sum()
         loss.backward()
         return loss, y0_t.grad, p_t.grad, stats
 
     stream = torch.cuda.current_stream(dev)
 
-    def timed(lu_precision, n_steps):
-        for _ in range(warmup):
-            value_and_grad(lu_precision)
+    def timed(lu_precision, n_steps, n_warm=None, **tighter):
+        for _ in range(warmup if n_warm is None else n_warm):
+            value_and_grad(lu_precision, **tighter)
         barrier(world)
         ms = []
         for _ in range(n_steps):
@@ -333,7 +333,7 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
             # tail of the one before.
             torch.cuda.synchronize(dev)
             e0.record(stream)
-            loss, gy, gp, stats = value_and_grad(lu_precision)
+            loss, gy, gp, stats = value_and_grad(lu_precision, **tighter)
             e1.record(stream)
             ms.append((e0, e1))
         barrier(world)
@@ -425,12 +425,22 @@ def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=Fals
         fms.append((e0, e1))
     barrier(world)
     fs_total = max_over_ranks(sum(a.elapsed_time(b) for a, b in fms), world)
+    # The adjoint at a tighter tolerance (rtol 1e-8, atol 1e-10): its error
+    # against the tight oracle gradient next to the forward sensitivities' at
+    # rtol 1e-6, so the two methods can be compared at matched error.
+    total_t, gy_t, gp_t, _ = timed("fp64", 1, n_warm=1, rtol=1e-8, atol=1e-10)
+    g_tight = torch.cat([gy_t, gp_t], dim=1)
+    result["adjoint_fp64_rtol_1e-8"] = {
+        "value": n * world / (total_t * 1e-3), "unit": "gradients/s", "ms_per_step": total_t,
+        "method": "the discrete adjoint, FP64, rtol 1e-8, atol 1e-10 (same loss and targets)",
+    }
     if oracle_checks and rank == 0 and world == 1:
         sample = 256
         result["error_vs_tight_oracle_gradient"] = gradient_errors(
             {"y0": cfg["y0"], "params": cfg["params"], "t_span": t}, target[:sample].cpu().numpy(),
             {"adjoint_fp64": g64[:sample].cpu().numpy(), "adjoint_fp32_lu": g32[:sample].cpu().numpy(),
-             "forward_sensitivities": g_fs[:sample].cpu().numpy()}, sample)
+             "forward_sensitivities": g_fs[:sample].cpu().numpy(),
+             "adjoint_fp64_rtol_1e-8": g_tight[:sample].cpu().numpy()}, sample)
     g_adj = torch.cat([gy, gp], dim=1)
     rel = ((g_adj - g_fs).abs().max(dim=1).values / g_fs.abs().max(dim=1).values.clamp_min(1e-300))
     result["forward_sensitivities"] = {

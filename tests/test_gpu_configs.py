@@ -23,6 +23,10 @@ Two bars:
   with its one-ulp-perturbed self (less a sampling margin), and its typical
   (median) trajectory difference must be of the size of the oracle's own
   rounding sensitivity.  A wrong kernel fails this by orders of magnitude.
+
+The product path (FP32 LU, fast arithmetic) is held to accuracy instead: its
+error against an FP64 oracle at rtol 1e-12 must be of the size of the FP64-LU
+solve's at the same tolerance.
 """
 
 import numpy as np
@@ -174,3 +178,45 @@ def test_gradient_config_full_horizon_within_rounding_noise(oracle, n_osc, count
     scale = np.abs(og).max(axis=1)
     _noise_bar(np.abs(g - og).max(axis=1) / scale, _same(stats, a, r),
                np.abs(pg - og).max(axis=1) / scale, (ap == a) & (rp == r), count)
+
+
+@pytest.mark.parametrize("n_osc,team", [(16, 0), (64, 8)], ids=["ring32_thread", "ring128_team8"])
+def test_vdp_ring_fp32_lu_as_accurate_as_fp64(oracle, n_osc, team):
+    """Configuration 3's product path -- FP32 LU, fast arithmetic, the autotuned
+    layout -- against a tight FP64 oracle (rtol 1e-12) over a few relaxation
+    cycles: each trajectory's worst error is of the size of the FP64-LU solve's at
+    the same tolerance (median and 90th percentile within 1.5x + 10 rtol, the
+    worst within 3x), the bar of the 8-state ring's test."""
+    cfg, y0, mu = _ring_inputs(n_osc, 64)
+    t_span = np.linspace(0.0, 30.0, 10)
+    h32 = rodas5P.solve(cfg["ode_fn"], y0, t_span, mu, rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp32",
+                        sparsity=cfg["sparsity"], team=team, launch="persistent")
+    system = oracle.System.vdp_ring(n_osc, 1.0, 0.1)
+    ref, *_ = oracle.solve("rodas5P", system, y0, t_span, mu, rtol=1e-12, atol=1e-14, lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, y0, t_span, mu, rtol=cfg["rtol"], atol=cfg["atol"],
+                           lu_precision="fp64")
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    err32 = (np.abs(h32 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    for q in (0.5, 0.9):
+        assert np.quantile(err32, q) <= 1.5 * np.quantile(err64, q) + 10 * cfg["rtol"]
+    assert err32.max() <= 3.0 * err64.max()
+
+
+@pytest.mark.parametrize("layout,team", [("sparse", 8), ("dense", 32)], ids=["team8_sparse", "team32_dense"])
+def test_brusselator_64_fp32_lu_config_horizon(oracle, layout, team):
+    """Configuration 4's product path (FP32 LU, fast arithmetic, the autotuned team
+    layouts) on its own inputs and horizon: within 1.5x the FP64-LU solve's error
+    against the rtol 1e-12 oracle, plus 10 rtol."""
+    cfg = systems.brusselator_config(n_grid=32, size=16384)
+    y0, b = cfg["y0"][:64], cfg["params"][:64]
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"])
+    h32 = rodas5P.solve(cfg["ode_fn"], y0, cfg["t_span"], b, lu_precision="fp32",
+                        sparsity=cfg["sparsity"] if layout == "sparse" else None, team=team, launch="persistent",
+                        **kw)
+    ref, *_ = oracle.solve("rodas5P", oracle.System.brusselator(32), y0, cfg["t_span"], b, rtol=1e-12,
+                           atol=1e-14, lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", oracle.System.brusselator(32), y0, cfg["t_span"], b, lu_precision="fp64",
+                           **kw)
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    assert (np.abs(h32 - ref) / scale).max() <= 1.5 * (np.abs(o64 - ref) / scale).max() + 10 * cfg["rtol"]

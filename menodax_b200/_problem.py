@@ -135,8 +135,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         raise ValueError("the team kernel runs Rodas5P")
     if options.team not in TEAM_SIZES:
         raise ValueError(f"team must be one of {TEAM_SIZES}; got {options.team}")
-    if options.sens is not None or options.save_hook is not None:
-        raise ValueError("the team kernel integrates the plain system: no sens or save_hook")
+    if options.sens is not None:
+        raise ValueError("the team kernel integrates the plain system: no forward sensitivities")
     if (options.checkpoint or options.adjoint) and options.sparsity is None:
         raise ValueError("the team kernel's checkpoints and reverse sweep need a sparse LU (a sparsity pattern)")
     tpb = int(options.threads_per_block)
@@ -204,7 +204,8 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         f"#define MDX_SAVE_HISTORY {1 if options.save_history else 0}",
         f"#define MDX_CHECKPOINT {1 if options.checkpoint else 0}",
         f"#define MDX_CKPT_SEG {int(options.ckpt_stride)}",
-        "#define MDX_HAS_HOOK 0",
+        f"#define MDX_HAS_HOOK {1 if options.save_hook is not None else 0}",
+        f"#define MDX_HOOK_SIZE {max(1, int(options.hook_size))}",
         f"#define MDX_FAST {1 if options.fast else 0}",
         f"#define MDX_TPB {tpb}",
         f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
@@ -218,8 +219,13 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
         "__device__ __forceinline__ double mdx_const_weight(int) { return 1.0; }",
         code.source,
         *extra,
-        '#include "mdx_team.cuh"',
     ]
+    hook_tables = []
+    if options.save_hook is not None:
+        hook = trace_hook(options.save_hook, n_vars, n_params, int(options.hook_size))
+        parts.append(emit_save_hook(hook))
+        hook_tables = hook.bounds()
+    parts.append('#include "mdx_team.cuh"')
     grad_bytes = 0
     if options.adjoint:
         grad_bytes = team_grad_slice_bytes(slice_size, n_vars, n_params, int(options.ckpt_stride),
@@ -230,7 +236,7 @@ def _build_team_source(tr, n_vars: int, n_params: int, options: KernelOptions, s
                 f"shared memory; use fewer threads per block")
         parts.append(emit_team_adjoint_functions(tr))
         parts.append('#include "mdx_team_adjoint.cuh"')
-    meta = dict(n_system=n_vars, n_error=n_vars, lu_size=lu_size, sparse=sparse, hook_tables=[],
+    meta = dict(n_system=n_vars, n_error=n_vars, lu_size=lu_size, sparse=sparse, hook_tables=hook_tables,
                 shared_bytes=shared, slice_bytes=slice_size, rhs_classes=code.n_rhs_classes,
                 jac_classes=code.n_jac_classes, grad_slice_bytes=grad_bytes)
     return "\n".join(parts) + "\n", meta

@@ -181,6 +181,16 @@ __device__ __forceinline__ void init(State& st, Slice& s, const Lanes& L, const 
   st.ckpt_overflow = false;
 #endif
   __syncwarp(L.mask);
+#if MDX_HAS_HOOK
+  // The hook (the thread kernel's generated code) runs on the team's first lane
+  // on the slice's state; its row starts at zero (modax/rodas5P.py:753-756).
+  if (L.lane == 0) {
+    double* acc = a.hook_out + (size_t)traj * MDX_HOOK_SIZE;
+    for (int j = 0; j < MDX_HOOK_SIZE; ++j) acc[j] = 0.0;
+    mdx_save_hook(0, s.y, t0, s.p, acc);
+  }
+  __syncwarp(L.mask);
+#endif
 }
 
 __device__ __forceinline__ bool running(const State& st, const MdxSolveArgs& a) {
@@ -350,6 +360,11 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
       const double theta = (a.times[st.save_idx] - t) / dt_use;
 #endif
       const double theta1 = 1.0 - theta;
+#if MDX_HAS_HOOK
+      // Every lane has read the error terms in f before any lane overwrites them
+      // with this save's state.
+      __syncwarp(L.mask);
+#endif
 #if MDX_FAST
       // The thread kernel's shared stage weights (mdx_rodas5p.cuh).
       double w[8];
@@ -378,10 +393,19 @@ __device__ __forceinline__ void step(State& st, Slice& s, const Lanes& L, const 
 #endif
 #if MDX_SAVE_HISTORY
         a.hist[hist_index(a, st.traj, st.save_idx, j)] = val;
+#endif
+#if MDX_HAS_HOOK
+        s.f[j] = val;  // the error terms in f are no longer needed
 #else
         (void)val;
 #endif
       }
+#if MDX_HAS_HOOK
+      __syncwarp(L.mask);
+      if (L.lane == 0)
+        mdx_save_hook(st.save_idx, s.f, a.times[st.save_idx], s.p, a.hook_out + (size_t)st.traj * MDX_HOOK_SIZE);
+      __syncwarp(L.mask);
+#endif
       ++st.save_idx;
     }
     for (int j = L.lane; j < MDX_NV; j += MDX_TEAM) s.y[j] = s.u[j] + (double)s.k[7][j];
@@ -400,6 +424,10 @@ __device__ __forceinline__ void finish(State& st, Slice& s, const Lanes& L, cons
   while (st.save_idx < a.n_save) {
 #if MDX_SAVE_HISTORY
     for (int j = L.lane; j < MDX_NV; j += MDX_TEAM) a.hist[hist_index(a, st.traj, st.save_idx, j)] = s.y[j];
+#endif
+#if MDX_HAS_HOOK
+    if (L.lane == 0)
+      mdx_save_hook(st.save_idx, s.y, a.times[st.save_idx], s.p, a.hook_out + (size_t)st.traj * MDX_HOOK_SIZE);
 #endif
     ++st.save_idx;
   }

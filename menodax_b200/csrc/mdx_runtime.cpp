@@ -344,8 +344,6 @@ int mdx_plan_create(const mdx_plan_desc* desc, mdx_plan** plan) {
   const int team = desc->team_size;
   if (team != 1 && team != 4 && team != 8 && team != 16 && team != 32)
     return fail(MDX_E_INVALID, "team_size must be 1, 4, 8, 16 or 32; got %d", team);
-  if (team > 1 && (desc->flags & MDX_PLAN_SAVE_HOOK))
-    return fail(MDX_E_INVALID, "a team module (team_size %d) has no save-hook kernels", team);
   if (desc->shared_bytes < 0 || desc->shared_bytes > MDX_MAX_SHARED_BYTES)
     return fail(MDX_E_INVALID, "shared_bytes must be in [0, %d]; got %d", MDX_MAX_SHARED_BYTES, desc->shared_bytes);
   mdx_plan* p = new (std::nothrow) mdx_plan;

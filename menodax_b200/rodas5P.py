@@ -93,8 +93,8 @@ def solve(
     ``16`` or ``32`` give each trajectory a team of that many lanes with its
     vectors and matrix in shared memory; ``"auto"`` leaves the choice to the
     launch autotuner, which considers teams for systems of
-    ``autotune.TEAM_MIN_VARS`` or more states.  Teams run no save hook and no
-    forward sensitivities; with a sparsity pattern and
+    ``autotune.TEAM_MIN_VARS`` or more states.  Teams run no forward
+    sensitivities; a save hook runs on a team's first lane; with a sparsity pattern and
     ``sens_error_control=False`` a team also runs the discrete adjoint (its
     checkpointing forward pass and its reverse sweep).
 
@@ -156,8 +156,6 @@ def solve(
 
     grad = needs_grad(y0, params)
     if team_choice:
-        if save_hook is not None:
-            raise ValueError("a team kernel solves the plain system: no save_hook")
         if grad and (sparsity is None or sens_error_control):
             raise ValueError("team gradients run the discrete adjoint over a sparse LU: pass a sparsity "
                              "pattern and sens_error_control=False")

@@ -53,11 +53,11 @@ def test_team_option_errors():
     with pytest.raises(ValueError, match="team must be"):
         rodas5P.solve(*args, team=3)
 
-    def hook(save_idx, y, t, p, acc):
-        acc[0] = acc[0] + y[0]
+    import torch
 
-    with pytest.raises(ValueError, match="save_hook"):
-        rodas5P.solve(*args, team=8, save_hook=hook, hook_size=1)
+    p_grad = torch.tensor(cfg["params"], requires_grad=True)
+    with pytest.raises(ValueError, match="sparsity pattern and sens_error_control=False"):
+        rodas5P.solve(cfg["ode_fn"], cfg["y0"], cfg["t_span"], p_grad, team=8)
     with pytest.raises(ValueError, match="whole warps"):
         rodas5P.solve(*args, team=8, trajectories_per_block=3)
 

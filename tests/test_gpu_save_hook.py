@@ -73,3 +73,25 @@ def test_hook_index_outside_its_row_is_refused_before_launch():
 
     with pytest.raises(ValueError, match="outside its"):
         rodas5P.solve(damped_oscillator, y0, t_span, params, save_hook=too_far, hook_size=N_SAVE)
+
+
+def test_team_kernel_runs_the_save_hook():
+    """The save hook in the team kernel (teams of 4 lanes on the 8-state VdP ring):
+    the same accumulation as the thread kernel's hook."""
+    from workloads import systems
+
+    cfg = systems.vdp_ring_config(4, size=64)
+    t_span = np.linspace(0.0, 5.0, 9)
+    weights = np.linspace(0.5, 1.5, 9)
+
+    def hook(save_idx, y, t, p_row, acc):
+        acc[0] += weights[save_idx] * y[0]
+        acc[1] += y[3] * y[3]
+        acc[2] += 1.0
+
+    kw = dict(rtol=1e-8, atol=1e-10, lu_precision="fp64", save_hook=hook, hook_size=3, launch="plain")
+    h0, a0 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], team=0, **kw)
+    h4, a4 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], team=4, **kw)
+    assert (a0[:, 2] == 9).all() and (a4[:, 2] == 9).all()
+    np.testing.assert_allclose(h4, h0, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(a4, a0, rtol=1e-9, atol=1e-12)

@@ -100,7 +100,7 @@ def _host_kernel(tmp_path, name, fn, n_vars, n_params, options):
     return lib
 
 
-def _solve(lib, y0, times, params, rtol, atol, max_steps=100000):
+def _solve(lib, y0, times, params, rtol, atol, max_steps=100000, hook_out=None):
     y0 = np.ascontiguousarray(y0, dtype=np.float64)
     times = np.ascontiguousarray(times, dtype=np.float64)
     params = np.ascontiguousarray(params, dtype=np.float64)
@@ -114,6 +114,8 @@ def _solve(lib, y0, times, params, rtol, atol, max_steps=100000):
     a.loop_steps, a.status = counters[2].ctypes.data, counters[3].ctypes.data
     a.n_traj, a.n_save, a.n_save_hist = n, len(times), len(times)
     a.max_steps, a.dt0, a.rtol, a.atol = max_steps, 0.0, rtol, atol
+    if hook_out is not None:
+        a.hook_out = hook_out.ctypes.data
     assert lib.run(a) == 0
     return hist, counters
 

@@ -325,3 +325,32 @@ def test_team_adjoint_matches_oracle_forward_sensitivities(tmp_path, oracle, str
         g32 = np.concatenate([gy32, gp32], axis=1)
         rel = np.abs(g32 - g64).max(axis=1) / np.abs(g64).max(axis=1)
         assert np.median(rel) < 1e-4
+
+
+def test_team_save_hook_matches_the_thread_kernel(tmp_path):
+    """A save hook in the team kernel (the generated hook code on the team's first
+    lane, at the initial state, every dense-output save and the frozen saves)
+    accumulates what the thread kernel's hook does (8-state VdP ring, teams of 4)."""
+    from test_kernel_host import _host_kernel
+
+    cfg = systems.vdp_ring_config(4, size=4)
+    t_span = np.linspace(0.0, 5.0, 9)
+    weights = np.linspace(0.5, 1.5, 9)
+
+    def hook(save_idx, y, t, p, acc):
+        acc[0] += weights[save_idx] * y[0]
+        acc[1] += y[3] * y[3]
+        acc[2] += 1.0
+
+    out = []
+    for team in (0, 4):
+        opts = KernelOptions(lu_precision="fp64", save_hook=hook, hook_size=3, team=team, threads_per_block=32)
+        lib = _team_kernel(tmp_path, "hook_team", cfg["ode_fn"], 8, 1, opts) if team else \
+            _host_kernel(tmp_path, "hook_thread", cfg["ode_fn"], 8, 1, opts)
+        hook_out = np.zeros((4, 3))
+        hist, counters = _solve(lib, cfg["y0"], t_span, cfg["params"], 1e-8, 1e-10, hook_out=hook_out)
+        out.append((hist, counters, hook_out))
+    (h0, c0, a0), (h4, c4, a4) = out
+    assert (c0[0] == c4[0]).all() and (a0[:, 2] == 9).all()
+    np.testing.assert_allclose(h4, h0, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(a4, a0, rtol=1e-9, atol=1e-12)

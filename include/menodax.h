@@ -109,6 +109,15 @@ typedef struct mdx_solve_desc {
   long long ckpt_capacity;
   int grid_blocks;        /* persistent: 0 = occupancy-sized */
   int reserved;
+  double* hist_host;      /* optional page-locked host copy of hist, same layout, or NULL.
+                             When set, the kernel copies each trajectory's history rows
+                             there as soon as they are final (a whole warp's contiguous
+                             rows at once in the one-trajectory-per-thread launch), so the
+                             transfer over the host link overlaps the trajectories still
+                             running; the host copy is complete when the stream is.  The
+                             buffer must lie inside one page-locked allocation the driver
+                             maps (cudaHostAlloc / cudaHostRegister): anything else is
+                             refused with MDX_E_INVALID before the launch. */
 } mdx_solve_desc;
 
 /* The reverse pass of the discrete adjoint over checkpoints a MDX_PLAN_CHECKPOINT

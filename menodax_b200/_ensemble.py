@@ -123,12 +123,15 @@ class Workspace:
 
 def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, mode,
            n_save_hist=None, grid_blocks=0, order=None, ckpt=None, ckpt_count=None,
-           ckpt_capacity=0, out=None, hook_out=None):
+           ckpt_capacity=0, out=None, hook_out=None, hist_host=None):
     """Allocate outputs on ``y0``'s device and launch one ensemble solve.
 
     All inputs must already be contiguous float64 CUDA tensors on one device.
     Returns ``(hist, counters)``; the rows of ``counters`` (4, N) int32 are the
     accepted, rejected and attempted step counts and the status bits.
+    ``hist_host`` (a pinned CPU tensor shaped like ``hist``) receives the
+    history from the kernel itself as trajectories finish; it is complete once
+    the launching stream is.
     """
     n = y0.shape[0]
     n_save = times.shape[0]
@@ -159,6 +162,11 @@ def launch(problem, *, y0, times, params, weights, dt0, rtol, atol, max_steps, m
     desc.status = counters[3].data_ptr()
     desc.order = order.data_ptr() if order is not None else None
     desc.hook_out = hook_out.data_ptr() if hook_out is not None else None
+    if hist_host is not None and n > 0:
+        if (hist_host.device.type != "cpu" or not hist_host.is_pinned() or hist_host.dtype != torch.float64
+                or tuple(hist_host.shape) != tuple(hist.shape) or not hist_host.is_contiguous()):
+            raise ValueError(f"hist_host must be a contiguous pinned float64 CPU tensor of shape {tuple(hist.shape)}")
+        desc.hist_host = hist_host.data_ptr()
     stream = torch.cuda.current_stream(dev).cuda_stream
     if mode == _native.MDX_LAUNCH_PERSISTENT:
         nbytes = problem.plan.workspace_size(mode, n)

@@ -98,14 +98,21 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
                 f"the save hook reads or writes {name} at save_idx + {hi if lo >= 0 else lo}, "
                 f"outside its {length} entries for {n_save} save times"
             )
-    hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, hook_out=hook_out, **common)
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
-    if torch_io and input_on_gpu:
+    hist_h = None
+    if not (torch_io and input_on_gpu):
+        # Host results: the kernel writes each finished trajectory's rows into
+        # pinned memory itself, so the transfer overlaps the rest of the solve.
+        hist_h = torch.empty((n, n_save if options.save_history else 1, problem.n_system),
+                             dtype=torch.float64, pin_memory=True)
+    hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, hook_out=hook_out,
+                            hist_host=hist_h, **common)
+    if hist_h is None:
         result = (hist,) if hook_out is None else (hist, hook_out)
         if return_stats:
             result += (solver_stats(counters[0], counters[1], counters[2], counters[3]),)
         return result[0] if len(result) == 1 else result
-    hist_h, counters_h = _to_host(hist, counters if return_stats else None)
+    counters_h = _to_host(hist, counters if return_stats else None)
     hook_h = None
     if hook_out is not None:
         hook_h = torch.empty(hook_out.shape, dtype=hook_out.dtype, pin_memory=True)
@@ -121,15 +128,14 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
 
 
 def _to_host(hist, counters):
-    """Device -> pinned host copies (torch's caching host allocator), one sync."""
-    hist_h = torch.empty(hist.shape, dtype=hist.dtype, pin_memory=True)
-    hist_h.copy_(hist, non_blocking=True)
+    """Copies the step counters to pinned host memory and waits for the stream,
+    which also completes the kernel's own writes of the history to the host."""
     counters_h = None
     if counters is not None:
         counters_h = torch.empty(counters.shape, dtype=counters.dtype, pin_memory=True)
         counters_h.copy_(counters, non_blocking=True)
     torch.cuda.current_stream(hist.device).synchronize()
-    return hist_h, counters_h
+    return counters_h
 
 
 def _replace(options, **kw):

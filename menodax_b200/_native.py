@@ -72,6 +72,7 @@ class SolveDesc(ctypes.Structure):
         ("workspace_bytes", ctypes.c_size_t), ("ckpt", ctypes.c_void_p),
         ("ckpt_count", ctypes.c_void_p), ("ckpt_capacity", ctypes.c_longlong),
         ("grid_blocks", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("hist_host", ctypes.c_void_p),
     ]
 
 

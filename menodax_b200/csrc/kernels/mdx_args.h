@@ -32,6 +32,7 @@ typedef struct MdxSolveArgs {
                               start states (ceil(capacity / MDX_CKPT_SEG), N, n_vars + 1) */
   int* ckpt_count;         /* adjoint forward pass: accepted steps recorded per trajectory */
   long long ckpt_capacity; /* steps per trajectory the checkpoint buffer holds */
+  double* hist_host;       /* page-locked host copy of hist (device-mapped address), or NULL */
   int n_traj;
   int n_save;
   int n_save_hist;         /* S, or 1 when only the final state is kept */

@@ -449,6 +449,14 @@ __device__ __forceinline__ void finish(State& st, Slice& s, const Lanes& L, cons
     if (a.status) a.status[st.traj] = status;
   }
   __syncwarp(L.mask);
+  if (a.hist_host != nullptr) {
+    // The team copies its finished row to the page-locked host copy; the barrier
+    // above ordered every lane's history stores before these L2 reads.
+    const size_t row = (size_t)a.n_save_hist * (size_t)MDX_NV;
+    const double* src = a.hist + (size_t)st.traj * row;
+    double* dst = a.hist_host + (size_t)st.traj * row;
+    for (size_t k = L.lane; k < row; k += MDX_TEAM) dst[k] = __ldcg(src + k);
+  }
 }
 
 }  // namespace team

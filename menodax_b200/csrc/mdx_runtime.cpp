@@ -64,6 +64,7 @@ struct Driver {
   decltype(&cuMemsetD32Async) memsetD32Async = nullptr;
   decltype(&cuOccupancyMaxActiveBlocksPerMultiprocessor) occupancy = nullptr;
   decltype(&cuGetErrorString) getErrorString = nullptr;
+  decltype(&cuPointerGetAttribute) pointerGetAttribute = nullptr;
 };
 
 Driver g_driver;
@@ -110,6 +111,7 @@ void load_driver() {
   resolve("cuMemsetD32Async", (void**)&g_driver.memsetD32Async);
   resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", (void**)&g_driver.occupancy);
   resolve("cuGetErrorString", (void**)&g_driver.getErrorString);
+  resolve("cuPointerGetAttribute", (void**)&g_driver.pointerGetAttribute);
   if (!all) return;
   if (g_driver.init(0) != CUDA_SUCCESS) {
     g_driver.why = "cuInit failed (no usable GPU)";
@@ -401,6 +403,35 @@ int mdx_occupancy(mdx_plan* plan, int mode, int* blocks_per_sm, int* sm_count) {
 
 }  // extern "C"
 
+namespace {
+
+// The device address of `bytes` of page-locked host memory at `p`, after
+// checking that the whole range lies inside one allocation the driver maps: a
+// kernel store to anything else would fault, so it is refused here instead.
+int host_mapping(const void* p, size_t bytes, double** device_address) {
+  const CUdeviceptr ptr = (CUdeviceptr)p;
+  unsigned int type = 0;
+  CUresult r = g_driver.pointerGetAttribute(&type, CU_POINTER_ATTRIBUTE_MEMORY_TYPE, ptr);
+  if (r != CUDA_SUCCESS || type != CU_MEMORYTYPE_HOST)
+    return fail(MDX_E_INVALID, "hist_host %p is not page-locked host memory the driver knows", p);
+  CUdeviceptr start = 0;
+  size_t size = 0;
+  if ((r = g_driver.pointerGetAttribute(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, ptr)) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuPointerGetAttribute(hist_host, RANGE_START_ADDR)");
+  if ((r = g_driver.pointerGetAttribute(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, ptr)) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuPointerGetAttribute(hist_host, RANGE_SIZE)");
+  if (ptr < start || bytes > size || ptr - start > size - bytes)
+    return fail(MDX_E_INVALID, "hist_host: %zu bytes at %p run past its page-locked allocation (%zu bytes at %p)",
+                bytes, p, size, (void*)start);
+  CUdeviceptr mapped = 0;
+  if ((r = g_driver.pointerGetAttribute(&mapped, CU_POINTER_ATTRIBUTE_DEVICE_POINTER, ptr)) != CUDA_SUCCESS)
+    return cuda_fail(r, "cuPointerGetAttribute(hist_host, DEVICE_POINTER)");
+  *device_address = (double*)mapped;
+  return MDX_OK;
+}
+
+}  // namespace
+
 namespace mdx_internal {
 
 // The body of mdx_solve.  `counter` (when not NULL) replaces the caller's
@@ -427,6 +458,13 @@ int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, in
     return fail(MDX_E_INVALID, "a checkpointing plan needs ckpt, ckpt_count and ckpt_capacity >= 1");
   if (d->mode == MDX_LAUNCH_PERSISTENT && !counter && (!d->workspace || d->workspace_bytes < 4))
     return fail(MDX_E_INVALID, "the persistent launch needs a workspace of at least 4 bytes");
+  double* hist_host = nullptr;
+  if (d->hist_host) {
+    int rc = require_driver();
+    if (rc) return rc;
+    const size_t bytes = (size_t)d->n_traj * (size_t)d->n_save_hist * (size_t)plan->desc.n_system * sizeof(double);
+    if ((rc = host_mapping(d->hist_host, bytes, &hist_host))) return rc;
+  }
 
   Loaded* l;
   int rc = load_for_context(plan, &l);
@@ -448,6 +486,7 @@ int solve_with_counter(mdx_plan* plan, const mdx_solve_desc* d, void* stream, in
   a.ckpt = ckpt ? d->ckpt : nullptr;
   a.ckpt_count = ckpt ? d->ckpt_count : nullptr;
   a.ckpt_capacity = ckpt ? d->ckpt_capacity : 0;
+  a.hist_host = hist_host;
   a.n_traj = d->n_traj;
   a.n_save = d->n_save;
   a.n_save_hist = d->n_save_hist;

@@ -44,6 +44,7 @@ static inline float host_powf(float a, float b) { return std::pow(a, b); }
 #define __fdividef host_fdividef
 #define __powf host_powf
 static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
+template <class T> static inline T __ldcg(const T* p) { return *p; }
 """
 
 DRIVER = """
@@ -68,7 +69,7 @@ class Args(ctypes.Structure):
                 ("rejected", ctypes.c_void_p), ("loop_steps", ctypes.c_void_p), ("status", ctypes.c_void_p),
                 ("hook_out", ctypes.c_void_p), ("work_counter", ctypes.c_void_p), ("order", ctypes.c_void_p),
                 ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p), ("ckpt_capacity", ctypes.c_longlong),
-                ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int), ("n_save_hist", ctypes.c_int),
+                ("hist_host", ctypes.c_void_p), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int), ("n_save_hist", ctypes.c_int),
                 ("max_steps", ctypes.c_int), ("dt0", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("atol", ctypes.c_double)]
 

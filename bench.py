@@ -464,13 +464,14 @@ def config_roofline(fn, n_vars, n_params, opts, counters, n, n_save, launch_ms, 
     import torch
 
     from menodax_b200._flops import rodas5p_cost, tsit5_cost
+    from menodax_b200._problem import wide_solve
     from menodax_b200._sparse_direct import sparse_lu_for
 
     if opts.solver == "tsit5":
         cost = tsit5_cost(fn, n_vars, n_params)
     else:
         sparse = sparse_lu_for(opts.sparsity, opts.ordering) if opts.sparsity is not None else None
-        cost = rodas5p_cost(fn, n_vars, n_params, sparse=sparse)
+        cost = rodas5p_cost(fn, n_vars, n_params, sparse=sparse, wide_solve=wide_solve(opts, n_vars))
     steps = float(counters[2].to(torch.float64).sum())
     f64 = steps * cost.f64 + n * (n_save - 1) * cost.per_save
     lu = steps * cost.lu
@@ -641,7 +642,7 @@ def main():
     from workloads import systems
     from menodax_b200._ensemble import launch
     from menodax_b200._flops import rodas5p_cost
-    from menodax_b200._problem import KernelOptions, get_problem
+    from menodax_b200._problem import KernelOptions, get_problem, wide_solve
 
     rank, world, local = dist_setup(args)
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -752,7 +753,7 @@ def main():
     clocks = sampler.stop() if sampler else {}
 
     # roofline of the timed kernel
-    cost = rodas5p_cost(fn, 3, 3)
+    cost = rodas5p_cost(fn, 3, 3, wide_solve=wide_solve(fast_opts, 3))
     peak64 = _native.measure_fma_peak(True)
     peak32 = _native.measure_fma_peak(False)
     per_launch_f64 = steps_done * cost.f64 + n_saves * cost.per_save

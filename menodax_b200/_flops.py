@@ -6,6 +6,8 @@ node by node from the traced graph, the LU, the solves and the stage algebra
 from the kernel's loop structure.  An FMA counts two.  FP32 operations are the
 LU-type work of an ``lu_precision="fp32"`` solve (substitutions, sparse
 updates, stored-stage conversions are not counted); everything else is FP64.
+With ``wide_solve`` (fast arithmetic on a small system) the substitutions run
+in FP64 against the FP32 factors, so only the factorisation is FP32 work.
 """
 
 from __future__ import annotations
@@ -39,7 +41,7 @@ class StepCost:
     per_save: int   # FP64 operations per dense-output save
 
 
-def rodas5p_cost(ode_fn, n_vars: int, n_params: int, *, sparse=None) -> StepCost:
+def rodas5p_cost(ode_fn, n_vars: int, n_params: int, *, sparse=None, wide_solve: bool = False) -> StepCost:
     tr = trace(ode_fn, n_vars, n_params)
     g = tr.graph
     rhs = _ops(g, tr.outputs)
@@ -72,6 +74,16 @@ def rodas5p_cost(ode_fn, n_vars: int, n_params: int, *, sparse=None) -> StepCost
         solve = 2 * subs + n
         lu_work = factor_lu + 8 * solve + n
         f64 = jac + 8 * rhs + stages + advance + error + controller + n
+    if wide_solve:
+        # The factorisation stays in the LU type (the fast dense LU runs there);
+        # the eight solves move to FP64.
+        solves = 8 * solve + n
+        if sparse is None:
+            f64 += solves - factor
+            lu_work = factor
+        else:
+            f64 += solves
+            lu_work = factor_lu
     per_save = ns * (3 * 15 + 9) + 4
     return StepCost(f64=f64, lu=lu_work, per_save=per_save)
 

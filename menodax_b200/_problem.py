@@ -105,6 +105,20 @@ def _sens_layout(n_vars, n_params, sens):
     return SensLayout(n_vars, n_params, n_y0_dirs, tuple(cols))
 
 
+# Fast arithmetic on systems up to this size solves in double against the FP32
+# factors (kernels/mdx_rodas5p.cuh, MDX_WIDE_SOLVE).
+WIDE_SOLVE_MAX_VARS = 8
+
+
+def wide_solve(options: KernelOptions, n_vars: int) -> bool:
+    """Whether a thread-kernel Rodas5P build solves its stages in double against
+    FP32 factors: fast arithmetic, ``lu_precision="fp32"``, at most
+    ``WIDE_SOLVE_MAX_VARS`` states (a joint sensitivity system follows its base
+    system, so its state rows match the plain solve's)."""
+    return (options.solver == "rodas5P" and not options.team and options.fast
+            and options.lu_precision == "fp32" and n_vars <= WIDE_SOLVE_MAX_VARS)
+
+
 def team_block_threads(n_vars: int, n_params: int, options: KernelOptions, preferred: int = 128) -> int:
     """Threads per block for a team launch: ``preferred`` or fewer, whole warps, and
     no more trajectories than a block's shared memory holds (a bound that assumes
@@ -299,6 +313,7 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
     e1, e2, e3 = controller_exponents(options)
     rodas = options.solver == "rodas5P"
     lu_t = "float" if options.lu_precision == "fp32" else "double"
+    wide = wide_solve(options, n_vars)
     parts = [
         f"// generated problem source: {options.solver}, n_vars={n_vars}, n_params={n_params}, n_sens={n_sens}",
         f"#define MDX_NV {n_vars}",
@@ -322,6 +337,8 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
         f"#define MDX_HOOK_SIZE {max(1, int(options.hook_size))}",
         f"#define MDX_TPB {int(options.threads_per_block)}",
         f"#define MDX_MIN_BLOCKS {int(options.min_blocks)}",
+        f"#define MDX_SOLVE_T {'double' if wide else lu_t}",
+        f"#define MDX_WIDE_SOLVE {1 if wide else 0}",
         '#include "mdx_common.cuh"',
     ]
     sens_weight = "1.0" if error_control else "0.0"
@@ -343,9 +360,9 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP& ipiv) "
                 "{ mdx::dense_factorize_fast<MDX_NV, MDX_LU_T>(lu, ipiv); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP& ipiv, R& rhs) "
-                "{ mdx::dense_solve_fast<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "{ mdx::dense_solve_fast<MDX_NV, MDX_SOLVE_T>(lu, ipiv, rhs); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP& ipiv, R& rhs) "
-                "{ mdx::dense_solve_t_fast<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "{ mdx::dense_solve_t_fast<MDX_NV, MDX_SOLVE_T>(lu, ipiv, rhs); }\n"
                 "__device__ __forceinline__ int mdx_diag_slot(int d) { return d * MDX_NV + d; }"
             )
         elif options.sparsity is None:
@@ -358,9 +375,9 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP& ipiv) "
                 "{ mdx::dense_factorize<MDX_NV, MDX_LU_T>(lu, ipiv); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP& ipiv, R& rhs) "
-                "{ mdx::dense_solve<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "{ mdx::dense_solve<MDX_NV, MDX_SOLVE_T>(lu, ipiv, rhs); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP& ipiv, R& rhs) "
-                "{ mdx::dense_solve_t<MDX_NV, MDX_LU_T>(lu, ipiv, rhs); }\n"
+                "{ mdx::dense_solve_t<MDX_NV, MDX_SOLVE_T>(lu, ipiv, rhs); }\n"
                 "__device__ __forceinline__ int mdx_diag_slot(int d) { return d * MDX_NV + d; }"
             )
         else:
@@ -376,9 +393,9 @@ def build_source(ode_fn, n_vars: int, n_params: int, options: KernelOptions):
                 "template <class LU, class IP> __device__ __forceinline__ void mdx_factorize(LU& lu, IP&) "
                 "{ mdx_sparse_factorize<MDX_LU_T>(lu); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve(const LU& lu, const IP&, R& rhs) "
-                "{ mdx_sparse_solve<MDX_LU_T>(lu, rhs); }\n"
+                "{ mdx_sparse_solve<MDX_SOLVE_T>(lu, rhs); }\n"
                 "template <class LU, class IP, class R> __device__ __forceinline__ void mdx_solve_t(const LU& lu, const IP&, R& rhs) "
-                "{ mdx_sparse_solve_t<MDX_LU_T>(lu, rhs); }\n"
+                "{ mdx_sparse_solve_t<MDX_SOLVE_T>(lu, rhs); }\n"
                 f"__device__ __forceinline__ int mdx_diag_slot(int d) {{ switch (d) {{ {cases} default: return 0; }} }}"
             )
         parts.append(emit_neg_jac(tr, structure, lu_size, sens))

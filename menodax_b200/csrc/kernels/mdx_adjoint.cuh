@@ -56,19 +56,29 @@ using namespace mdx::rodas5p;
 // forward step did (the same 1/h and 1/(h gamma), step_reciprocals): the
 // factorised iteration matrix, the eight stages and the point each stage's f was
 // evaluated at.  The end state is us[7] + k[7].
-template <class LU, class IP, class K, class US, class DTV>
+// `lus` receives the matrix the solves use: the factors, or (MDX_WIDE_SOLVE)
+// their widened copy, as in the forward step.
+template <class SLU, class IP, class K, class US, class DTV>
 __device__ __forceinline__ void recompute(double t, double h, const double (&y)[MDX_NV], const double* p,
-                                          LU& lu, IP& ipiv, K& k, US& us, DTV& dT) {
+                                          SLU& lus, IP& ipiv, K& k, US& us, DTV& dT) {
   typedef MDX_LU_T T;
   double inv_dt, dtgamma_inv;
   step_reciprocals(h, inv_dt, dtgamma_inv);
   const double t_end = t + h;
+#if MDX_WIDE_SOLVE
+  T lu[MDX_LU_SIZE];
+#else
+  SLU& lu = lus;
+#endif
   mdx_neg_jac(y, t, p, lu, dT);
 #pragma unroll
   for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (T)dtgamma_inv;
   mdx_factorize(lu, ipiv);
+#if MDX_WIDE_SOLVE
+  widen_factors(lu, lus);
+#endif
   double u[MDX_NV], work[MDX_NV];
-  T rhs[MDX_NV];
+  sol_t rhs[MDX_NV];
   const double tstage[8] = {t, t + coef_ct(0) * h, t + coef_ct(1) * h, t + coef_ct(2) * h,
                             t + coef_ct(3) * h, t_end, t_end, t_end};
 #pragma unroll
@@ -103,9 +113,9 @@ __device__ __forceinline__ void recompute(double t, double h, const double (&y)[
         if (coef_d(s) != 0.0 && !MDX_AUTONOMOUS) value = work[j] + h * coef_d(s) * dT[j] + acc * inv_dt;
         else value = work[j] + acc * inv_dt;
       }
-      rhs[j] = (T)value;
+      rhs[j] = (sol_t)value;
     }
-    mdx_solve(lu, ipiv, rhs);
+    mdx_solve(lus, ipiv, rhs);
 #pragma unroll
     for (int j = 0; j < MDX_NV; ++j) k[s][j] = rhs[j];
   }
@@ -114,9 +124,9 @@ __device__ __forceinline__ void recompute(double t, double h, const double (&y)[
 // The end state of one accepted step, for replaying a segment forward.
 __device__ __forceinline__ void replay_step(double t, double h, const double (&y)[MDX_NV], const double* p,
                                             double (&y_next)[MDX_NV]) {
-  MDX_LU_T lu[MDX_LU_SIZE];
+  sol_t lu[MDX_LU_SIZE];
   int ipiv[MDX_IPIV];
-  MDX_LU_T k[8][MDX_NV];
+  sol_t k[8][MDX_NV];
   double us[8][MDX_NV];
   double dT[MDX_NV];
   recompute(t, h, y, p, lu, ipiv, k, us, dT);
@@ -131,13 +141,12 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
                                              const double (&y)[MDX_NV], const double* p,
                                              int s_lo, int s_hi, double (&ybar)[MDX_NV],
                                              double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
-  typedef MDX_LU_T T;
   double inv_dt, dtgamma_inv;
   step_reciprocals(h, inv_dt, dtgamma_inv);
   const double t_end = t + h;
-  T lu[MDX_LU_SIZE];
+  sol_t lu[MDX_LU_SIZE];
   int ipiv[MDX_IPIV];
-  T k[8][MDX_NV];
+  sol_t k[8][MDX_NV];
   double us[8][MDX_NV];
   double dT[MDX_NV];
   recompute(t, h, y, p, lu, ipiv, k, us, dT);
@@ -191,9 +200,9 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 
 #pragma unroll
   for (int s = 7; s >= 0; --s) {
-    T rb_t[MDX_NV];
+    sol_t rb_t[MDX_NV];
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) rb_t[j] = (T)kbar[s][j];
+    for (int j = 0; j < MDX_NV; ++j) rb_t[j] = (sol_t)kbar[s][j];
     mdx_solve_t(lu, ipiv, rb_t);
     double rbar[MDX_NV];
 #pragma unroll

@@ -31,14 +31,36 @@ typedef MDX_LU_T lu_t;
 #ifndef MDX_AUTONOMOUS
 #define MDX_AUTONOMOUS 0
 #endif
-// The stage increments are rounded to the LU type when stored (the reference's
-// k_stages, modax/rodas5P.py:724).  Small systems keep the rounded values in
-// double registers, which holds the same numbers without converting on every use.
-#if MDX_NS <= 8
+// The triangular solves' type.  The reference solves in the LU type and rounds
+// the stage increments to it (k_stages, modax/rodas5P.py:724), and so do the
+// reference arithmetic and every large system here.  Fast arithmetic on a
+// system of up to 8 states (MDX_WIDE_SOLVE) factorises in FP32 as well but
+// solves in double against the factors, widened once per step: one conversion
+// per factor entry instead of two per component and stage, which on the B200's
+// half-rate FP64 pipe costs less than the conversions it replaces, and the
+// stages keep their full double values.
+#ifndef MDX_SOLVE_T
+#define MDX_SOLVE_T MDX_LU_T
+#endif
+#ifndef MDX_WIDE_SOLVE
+#define MDX_WIDE_SOLVE 0
+#endif
+typedef MDX_SOLVE_T sol_t;
+// Stage increments: small systems keep them in double registers (the rounded
+// values, or the wide solve's own), larger ones in the LU type.
+#if MDX_NS <= 8 || MDX_WIDE_SOLVE
 typedef double k_t;
 #else
 typedef lu_t k_t;
 #endif
+
+// The matrix the stages solve against: the factors themselves, or their
+// widened copy.
+template <class LU, class SLU>
+__device__ __forceinline__ void widen_factors(const LU& lu, SLU& lus) {
+#pragma unroll
+  for (int i = 0; i < MDX_LU_SIZE; ++i) lus[i] = (sol_t)lu[i];
+}
 
 struct State {
   double y[MDX_NS];
@@ -130,7 +152,7 @@ __device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& 
         value = work[j] + acc * inv_dt;
       }
     }
-    if (j < MDX_NV) rhs[j] = (lu_t)value;
+    if (j < MDX_NV) rhs[j] = (sol_t)value;
     else work[j] = value;
   }
   mdx_solve(lu, ipiv, rhs);
@@ -146,7 +168,7 @@ __device__ __forceinline__ void stage(const LU& lu, const IP& ipiv, RB& rhs, K& 
   for (int s = 0; s < MDX_NSENS; ++s) {
     const int base = MDX_NV + s * MDX_NV;
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) rhs[j] = (lu_t)(work[base + j] + coupling[s * MDX_NV + j]);
+    for (int j = 0; j < MDX_NV; ++j) rhs[j] = (sol_t)(work[base + j] + coupling[s * MDX_NV + j]);
     mdx_solve(lu, ipiv, rhs);
 #pragma unroll
     for (int j = 0; j < MDX_NV; ++j) k[S][base + j] = (k_t)rhs[j];
@@ -193,37 +215,43 @@ __device__ __forceinline__ void step(State& st, const MdxSolveArgs& a) {
 #pragma unroll
   for (int d = 0; d < MDX_NV; ++d) lu[mdx_diag_slot(d)] += (lu_t)dtgamma_inv;
   mdx_factorize(lu, ipiv);
+#if MDX_WIDE_SOLVE
+  sol_t lus[MDX_LU_SIZE];
+  widen_factors(lu, lus);
+#else
+  lu_t (&lus)[MDX_LU_SIZE] = lu;
+#endif
 
-  lu_t rhs[MDX_NV];
+  sol_t rhs[MDX_NV];
   k_t k[8][MDX_NS];
   double u[MDX_NS];
   double work[MDX_NS];
 
   mdx_rhs(st.y, t, st.p, work);
-  stage<0>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<0>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
   advance<0>(u, st, k);
   mdx_rhs(u, t + coef_ct(0) * dt_use, st.p, work);
-  stage<1>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<1>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
   advance<1>(u, st, k);
   mdx_rhs(u, t + coef_ct(1) * dt_use, st.p, work);
-  stage<2>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<2>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
   advance<2>(u, st, k);
   mdx_rhs(u, t + coef_ct(2) * dt_use, st.p, work);
-  stage<3>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<3>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
   advance<3>(u, st, k);
   mdx_rhs(u, t + coef_ct(3) * dt_use, st.p, work);
-  stage<4>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<4>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
   advance<4>(u, st, k);
   mdx_rhs(u, t_end, st.p, work);
-  stage<5>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<5>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
 #pragma unroll
   for (int j = 0; j < MDX_NS; ++j) u[j] += (double)k[5][j];
   mdx_rhs(u, t_end, st.p, work);
-  stage<6>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<6>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
 #pragma unroll
   for (int j = 0; j < MDX_NS; ++j) u[j] += (double)k[6][j];
   mdx_rhs(u, t_end, st.p, work);
-  stage<7>(lu, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
+  stage<7>(lus, ipiv, rhs, k, work, dT, st, dt_use, inv_dt);
 
   // Weighted RMS of the embedded error estimate k8 (modax/rodas5P.py:903-911).
   double err_local = 0.0;

@@ -69,8 +69,8 @@ class Args(ctypes.Structure):
                 ("rejected", ctypes.c_void_p), ("loop_steps", ctypes.c_void_p), ("status", ctypes.c_void_p),
                 ("hook_out", ctypes.c_void_p), ("work_counter", ctypes.c_void_p), ("order", ctypes.c_void_p),
                 ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p), ("ckpt_capacity", ctypes.c_longlong),
-                ("hist_host", ctypes.c_void_p), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int), ("n_save_hist", ctypes.c_int),
-                ("max_steps", ctypes.c_int), ("dt0", ctypes.c_double), ("rtol", ctypes.c_double),
+                ("hist_host", ctypes.c_void_p), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int),
+                ("n_save_hist", ctypes.c_int), ("max_steps", ctypes.c_int), ("dt0", ctypes.c_double), ("rtol", ctypes.c_double),
                 ("atol", ctypes.c_double)]
 
 
@@ -315,6 +315,36 @@ def test_adjoint_matches_oracle_forward_sensitivities(tmp_path, oracle, solver, 
     for got, ref in ((gy, oy), (gp, op)):
         scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
         assert (np.abs(got - ref) / scale).max() < 1e-7
+
+
+@pytest.mark.parametrize("layout", ["dense", "sparse"])
+def test_wide_solve_adjoint_replays_the_forward_steps_exactly(tmp_path, layout):
+    """Fast arithmetic with FP32 LUs on a small system solves in double against
+    the widened factors.  The reverse sweep's recompute must do the same: with a
+    checkpoint every 8 steps it replays 7 of each 8 steps from the segment's
+    start, with a checkpoint every step it replays none.  The two gradients agree
+    to the last few ulps (contraction of the two code paths differs) when a
+    replayed step is the forward step; a replay that solved in FP32 would put
+    them ~1e-7 apart."""
+    from menodax_b200._problem import wide_solve
+
+    n_osc = 3
+    cfg = systems.vdp_gradient_config(n_osc, size=16)
+    t_span = np.linspace(0.0, 5.0, 6)
+    pattern = normalize_sparsity(systems.vdp_sparsity(n_osc), 2 * n_osc) if layout == "sparse" else None
+    w = np.random.default_rng(12).normal(size=(16, len(t_span), 2 * n_osc))
+    out = {}
+    for stride in (1, 8):
+        options = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern, checkpoint=True, adjoint=True,
+                                ckpt_stride=stride)
+        assert wide_solve(options, 2 * n_osc)
+        lib = _host_adjoint(tmp_path, f"wide_{layout}_{stride}", cfg["ode_fn"], 2 * n_osc, 1, options)
+        out[stride] = _value_and_grad(lib, cfg["y0"], t_span, cfg["params"], w, 1e-6, 1e-8, stride,
+                                      capacity=4096)
+    assert np.array_equal(out[1][0], out[8][0])
+    for a, b in zip(out[1][1:], out[8][1:]):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+    assert np.abs(out[1][1]).max() > 0.0
 
 
 def test_rodas5p_time_derivative_and_tf_index(tmp_path):

@@ -100,19 +100,23 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
             )
     input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     hist_h = None
+    streamed = False
     if not (torch_io and input_on_gpu):
-        # Host results: the kernel writes each finished trajectory's rows into
-        # pinned memory itself, so the transfer overlaps the rest of the solve.
         hist_h = torch.empty((n, n_save if options.save_history else 1, problem.n_system),
                              dtype=torch.float64, pin_memory=True)
+        # Host results of a one-launch solve: each warp (or team) writes its
+        # finished rows into the pinned buffer itself, overlapping the rest of the
+        # solve.  The persistent launch finishes one lane's row at a time, too
+        # small a write for the host link, so its history is copied afterwards.
+        streamed = mode == _native.MDX_LAUNCH_PLAIN
     hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, hook_out=hook_out,
-                            hist_host=hist_h, **common)
+                            hist_host=hist_h if streamed else None, **common)
     if hist_h is None:
         result = (hist,) if hook_out is None else (hist, hook_out)
         if return_stats:
             result += (solver_stats(counters[0], counters[1], counters[2], counters[3]),)
         return result[0] if len(result) == 1 else result
-    counters_h = _to_host(hist, counters if return_stats else None)
+    counters_h = _to_host(hist, None if streamed else hist_h, counters if return_stats else None)
     hook_h = None
     if hook_out is not None:
         hook_h = torch.empty(hook_out.shape, dtype=hook_out.dtype, pin_memory=True)
@@ -127,9 +131,11 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     return result[0] if len(result) == 1 else result
 
 
-def _to_host(hist, counters):
-    """Copies the step counters to pinned host memory and waits for the stream,
-    which also completes the kernel's own writes of the history to the host."""
+def _to_host(hist, hist_h, counters):
+    """Copies the history (unless the kernel wrote it to ``hist_h`` itself) and
+    the step counters to pinned host memory, and waits for the stream."""
+    if hist_h is not None:
+        hist_h.copy_(hist, non_blocking=True)
     counters_h = None
     if counters is not None:
         counters_h = torch.empty(counters.shape, dtype=counters.dtype, pin_memory=True)

@@ -1,12 +1,14 @@
 """The history written to pinned host memory by the solve kernel itself.
 
-Host results (NumPy or CPU-tensor inputs) come back through
-``mdx_solve_desc.hist_host``: each warp, or each team, copies its finished
-trajectories' rows across the host link while the rest of the ensemble still
-steps.  The host copy must equal the device history bit for bit, for both
-launch shapes, ragged ensembles (a partial last warp), the final-state-only
-history and the team kernel; the runtime must refuse host memory the kernel
-cannot reach before it launches anything.
+Host results (NumPy or CPU-tensor inputs) of a one-launch solve come back
+through ``mdx_solve_desc.hist_host``: each warp, or each team, copies its
+finished trajectories' rows across the host link while the rest of the ensemble
+still steps (the persistent launch's results are copied after the kernel by the
+Python front end, and its in-kernel copy is reached through the C ABI).  The
+host copy must equal the device history bit for bit, for both launch shapes,
+ragged ensembles (a partial last warp), the final-state-only history and the
+team kernel; the runtime must refuse host memory the kernel cannot reach before
+it launches anything.
 """
 
 import ctypes
@@ -18,6 +20,7 @@ import torch
 from menodax_b200 import _native, rodas5P, tsit5
 from menodax_b200._ensemble import launch
 from menodax_b200._problem import KernelOptions, get_problem
+from menodax_b200._sparsity import normalize_sparsity
 from workloads import systems
 
 pytestmark = pytest.mark.gpu
@@ -102,6 +105,23 @@ def test_host_copy_with_stats_and_cpu_tensors():
                                    atol=cfg["atol"], return_stats=True)
     assert torch.equal(hist, ref.cpu())
     assert torch.equal(torch.as_tensor(stats["accepted_steps"]), ref_stats["accepted_steps"].cpu())
+
+
+@pytest.mark.parametrize("team", [0, 4])
+def test_persistent_kernels_copy_rows_through_the_abi(team):
+    cfg = systems.vdp_ring_config(4, size=777)
+    dev = torch.device("cuda", 0)
+    t_span = np.linspace(0.0, 30.0, 20)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=normalize_sparsity(cfg["sparsity"], 8),
+                         team=team, threads_per_block=64)
+    problem = get_problem(cfg["ode_fn"], 8, 1, opts)
+    kw = dict(y0=torch.as_tensor(cfg["y0"], device=dev), times=torch.as_tensor(t_span, device=dev),
+              params=torch.as_tensor(cfg["params"], device=dev), weights=None, dt0=0.0, rtol=1e-6, atol=1e-8,
+              max_steps=100000, mode=_native.MDX_LAUNCH_PERSISTENT)
+    host = torch.zeros((777, len(t_span), 8), dtype=torch.float64, pin_memory=True)
+    hist, _ = launch(problem, hist_host=host, **kw)
+    torch.cuda.synchronize()
+    assert torch.equal(host, hist.cpu())
 
 
 def _robertson_launch_args(n):

@@ -553,11 +553,8 @@ def measure_config(name, steps, warmup, rank, world, *, max_steps=100000, n_limi
         else:
             choice = autotune.tune(fn, n_vars, n_params, opts, tune_team=True,
                                    tune_shared=opts.solver == "tsit5", **common)
-            from dataclasses import replace
-
-            prob = get_problem(fn, n_vars, n_params,
-                               replace(opts, threads_per_block=choice.threads_per_block, team=choice.team,
-                                       shared_stages=choice.shared_stages))
+            opts = autotune.options_for(opts, choice)
+            prob = get_problem(fn, n_vars, n_params, opts)
             mode, grid = choice.mode, autotune.grid_blocks(prob, choice, n)
             label = choice.describe()
         # Warm up for the requested launches and at least WARM_S of device work:
@@ -701,8 +698,7 @@ def main():
     fast_opts = KernelOptions(lu_precision="fp32", fast=True)
     choice = autotune.tune(fn, 3, 3, fast_opts, y0=y0, times=times, params=params, weights=None,
                            dt0=0.0, rtol=cfg["rtol"], atol=cfg["atol"], max_steps=100000)
-    tuned = get_problem(fn, 3, 3, KernelOptions(lu_precision="fp32", fast=True,
-                                                threads_per_block=choice.threads_per_block))
+    tuned = get_problem(fn, 3, 3, autotune.options_for(fast_opts, choice))
     tuned_grid = autotune.grid_blocks(tuned, choice, n)
     for prob, mode in ((tuned, choice.mode), (fp32, _native.MDX_LAUNCH_PERSISTENT),
                        (fp64, _native.MDX_LAUNCH_PLAIN), (fp32_ref, _native.MDX_LAUNCH_PLAIN)):

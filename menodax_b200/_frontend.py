@@ -84,8 +84,7 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
 
         choice = autotune.tune(ode_fn, n_vars, n_params, options, tune_block=tune_block,
                                tune_team=tune_team, tune_shared=tune_shared, **common)
-        options = _replace(options, threads_per_block=choice.threads_per_block, team=choice.team,
-                           shared_stages=choice.shared_stages)
+        options = autotune.options_for(options, choice)
         problem = get_problem(ode_fn, n_vars, n_params, options)
         mode = choice.mode
         grid_blocks = autotune.grid_blocks(problem, choice, n)

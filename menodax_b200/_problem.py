@@ -72,6 +72,9 @@ class KernelOptions:
     # Rodas5P: an array-form right-hand side array_rhs(y, t, p, out) for the stage
     # evaluations; derivatives still come from ode_fn (modax/rodas5P.py:382-391).
     array_rhs: object = None
+    # Fast FP32-LU thread kernels: solve the stages in double against the
+    # widened factors (True) or in FP32 (False); None picks by size (wide_solve).
+    wide_solve: bool | None = None
 
 
 def controller_exponents(options: KernelOptions):
@@ -106,17 +109,27 @@ def _sens_layout(n_vars, n_params, sens):
 
 
 # Fast arithmetic on systems up to this size solves in double against the FP32
-# factors (kernels/mdx_rodas5p.cuh, MDX_WIDE_SOLVE).
+# factors by default (kernels/mdx_rodas5p.cuh, MDX_WIDE_SOLVE); larger thread
+# kernels keep FP32 solves unless the autotuner measured the wide ones faster.
 WIDE_SOLVE_MAX_VARS = 8
+
+
+def wide_solve_applies(options: KernelOptions) -> bool:
+    """Whether the build has the choice at all: a fast FP32-LU Rodas5P thread kernel."""
+    return (options.solver == "rodas5P" and not options.team and options.fast
+            and options.lu_precision == "fp32")
 
 
 def wide_solve(options: KernelOptions, n_vars: int) -> bool:
     """Whether a thread-kernel Rodas5P build solves its stages in double against
-    FP32 factors: fast arithmetic, ``lu_precision="fp32"``, at most
+    FP32 factors: ``options.wide_solve`` when set, else for systems of at most
     ``WIDE_SOLVE_MAX_VARS`` states (a joint sensitivity system follows its base
     system, so its state rows match the plain solve's)."""
-    return (options.solver == "rodas5P" and not options.team and options.fast
-            and options.lu_precision == "fp32" and n_vars <= WIDE_SOLVE_MAX_VARS)
+    if not wide_solve_applies(options):
+        return False
+    if options.wide_solve is not None:
+        return bool(options.wide_solve)
+    return n_vars <= WIDE_SOLVE_MAX_VARS
 
 
 def team_block_threads(n_vars: int, n_params: int, options: KernelOptions, preferred: int = 128) -> int:

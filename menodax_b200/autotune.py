@@ -10,7 +10,10 @@ launch) on the caller's own inputs -- or on a leading sample of them for large
 ensembles -- and the fastest is remembered per (problem, ensemble size, device).
 
 Candidates: plain and persistent launches at 32, 64 and 128 threads per block,
-the persistent grid at the occupancy limit or half of it; for systems of
+the persistent grid at the occupancy limit or half of it; for fast FP32-LU
+thread kernels of 9 to ``WIDE_TUNE_MAX_VARS`` states, each of those with the
+stage solves in FP32 and in FP64 against the widened factors (which wins
+depends on what the larger vectors do to register spills); for systems of
 ``TEAM_MIN_VARS`` states or more, also the team kernel (a team of 8 to 32 lanes
 per trajectory, its vectors and matrix in shared memory), plain and persistent.
 The thread kernel is a candidate up to ``THREAD_MAX_VARS`` states with a sparse
@@ -42,9 +45,11 @@ from menodax_b200._ensemble import launch
 from menodax_b200._problem import (
     DENSE_UNROLL_MAX,
     STATIC_SHARED_MAX,
+    WIDE_SOLVE_MAX_VARS,
     get_problem,
     team_block_threads,
     tsit5_stage_bytes,
+    wide_solve_applies,
 )
 from menodax_b200._team import TEAM_SIZES
 
@@ -56,6 +61,7 @@ BUDGET_S = 3.0
 TEAM_MIN_VARS = 16
 SHARED_STAGES_MAX_VARS = 16   # the reference's bound for its shared Tsit5 backend
 THREAD_MAX_VARS = 128
+WIDE_TUNE_MAX_VARS = 64
 
 
 @dataclass(frozen=True)
@@ -65,12 +71,22 @@ class LaunchChoice:
     grid_fill: float  # persistent: fraction of the occupancy-limited grid
     team: int = 0     # lanes per trajectory; 0 = one thread per trajectory
     shared_stages: bool = False  # Tsit5: stage vectors in shared memory
+    wide_solve: bool | None = None  # fast FP32-LU thread kernels: FP64 stage solves; None = by size
 
     def describe(self) -> str:
         kind = "plain" if self.mode == _native.MDX_LAUNCH_PLAIN else f"persistent(fill={self.grid_fill})"
         lanes = f", team of {self.team}" if self.team else ""
         stages = ", stages in shared memory" if self.shared_stages else ""
-        return f"{kind}, {self.threads_per_block} threads/block{lanes}{stages}"
+        solves = "" if self.wide_solve is None else (", FP64 solves" if self.wide_solve else ", FP32 solves")
+        return f"{kind}, {self.threads_per_block} threads/block{lanes}{stages}{solves}"
+
+
+def options_for(options, choice: LaunchChoice):
+    """``options`` with the launch choice's block size, team, stage placement and
+    solve type."""
+    return replace(options, threads_per_block=choice.threads_per_block, team=choice.team,
+                   shared_stages=choice.shared_stages,
+                   wide_solve=options.wide_solve if choice.wide_solve is None else choice.wide_solve)
 
 
 
@@ -79,14 +95,16 @@ _cache: dict = {}
 _lock = threading.Lock()
 
 
-def candidates(block_sizes=BLOCK_SIZES, teams=(), shared_blocks=(), shared_default=False):
-    """Thread-kernel launches per block size; team launches as ``(team, threads_per_block)``
-    pairs; Tsit5 launches with shared-memory stages per block size in ``shared_blocks``."""
+def candidates(block_sizes=BLOCK_SIZES, teams=(), shared_blocks=(), shared_default=False, solves=(None,)):
+    """Thread-kernel launches per block size (and per stage-solve type in
+    ``solves``); team launches as ``(team, threads_per_block)`` pairs; Tsit5
+    launches with shared-memory stages per block size in ``shared_blocks``."""
     out = []
-    for tpb in block_sizes:
-        out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, 0, shared_default))
-        for fill in PERSISTENT_FILL:
-            out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill, 0, shared_default))
+    for wide in solves:
+        for tpb in block_sizes:
+            out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, 0, shared_default, wide))
+            for fill in PERSISTENT_FILL:
+                out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PERSISTENT, fill, 0, shared_default, wide))
     for tpb in shared_blocks:
         out.append(LaunchChoice(tpb, _native.MDX_LAUNCH_PLAIN, 0.0, 0, True))
         for fill in PERSISTENT_FILL:
@@ -165,7 +183,11 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
     shared_blocks = ()
     if tune_shared and options.solver == "tsit5" and not options.shared_stages and n_vars <= SHARED_STAGES_MAX_VARS:
         shared_blocks = tuple(b for b in blocks if tsit5_stage_bytes(n_vars, b) <= STATIC_SHARED_MAX)
-    cands = candidates(blocks, teams, shared_blocks, options.shared_stages)
+    solves = (None,)
+    if (wide_solve_applies(options) and options.wide_solve is None
+            and WIDE_SOLVE_MAX_VARS < n_vars <= WIDE_TUNE_MAX_VARS):
+        solves = (False, True)
+    cands = candidates(blocks, teams, shared_blocks, options.shared_stages, solves)
     key = (ode_fn, n_vars, n_params, replace(options, threads_per_block=32, team=0, shared_stages=False), n,
            tuple(cands), max_steps, torch.cuda.get_device_name(y0.device))
     with _lock:
@@ -174,9 +196,7 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
         return found
 
     def problem_for(choice):
-        return get_problem(ode_fn, n_vars, n_params,
-                           replace(options, threads_per_block=choice.threads_per_block, team=choice.team,
-                                   shared_stages=choice.shared_stages))
+        return get_problem(ode_fn, n_vars, n_params, options_for(options, choice))
 
     buildable = []
     for choice in cands:
@@ -209,7 +229,7 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
         fill = 1.0 if winner.team else 0.5
         persistent = [c for c in buildable if c.mode == _native.MDX_LAUNCH_PERSISTENT and c.team == winner.team
                       and c.threads_per_block == winner.threads_per_block and c.grid_fill == fill
-                      and c.shared_stages == winner.shared_stages]
+                      and c.shared_stages == winner.shared_stages and c.wide_solve == winner.wide_solve]
         choice = persistent[0] if persistent else winner
         with _lock:
             _cache[key] = choice

@@ -10,7 +10,6 @@ buffers and replays the graph.  The launch shape is the autotuned one.
 
 from __future__ import annotations
 
-from dataclasses import replace
 
 import numpy as np
 import torch
@@ -68,8 +67,8 @@ class GraphedSolve:
             choice = autotune.tune(self._ode_fn, n_vars, n_params, opts, **self._common)
         else:
             mode = _native.MDX_LAUNCH_PERSISTENT if self._launch_mode == "persistent" else _native.MDX_LAUNCH_PLAIN
-            choice = autotune.LaunchChoice(opts.threads_per_block, mode, 1.0)
-        problem = get_problem(self._ode_fn, n_vars, n_params, replace(opts, threads_per_block=choice.threads_per_block))
+            choice = autotune.LaunchChoice(opts.threads_per_block, mode, 1.0, opts.team, opts.shared_stages)
+        problem = get_problem(self._ode_fn, n_vars, n_params, autotune.options_for(opts, choice))
         grid = autotune.grid_blocks(problem, choice, n)
         kw = dict(mode=choice.mode, grid_blocks=grid, out=(self.hist, self.counters), **self._common)
         self.launch_choice = choice

@@ -138,3 +138,25 @@ def test_tsit5_auto_backend_times_shared_stage_launches(fake_device, monkeypatch
     rec = Recorder(lambda c, m, s: 1.0, steps=10)
     _tune(fn, 16, opts, rec, monkeypatch, tune_shared=False)
     assert not any(c.shared_stages for c, _, _ in rec.calls)
+
+
+def test_fp64_stage_solves_are_a_candidate_for_mid_sized_thread_kernels(fake_device, monkeypatch):
+    """Fast FP32-LU thread kernels of 9-64 states are timed with the stage solves
+    in FP32 and in FP64 against the widened factors; smaller systems take the
+    FP64 solves without timing, teams and FP64 LUs never have the choice."""
+    fn, n, pattern = _ring(16)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern)
+    rec = Recorder(lambda c, m, s: 0.5 if c.wide_solve else 1.0, steps=10)
+    choice = _tune(fn, n, opts, rec, monkeypatch)
+    assert {c.wide_solve for c, _, _ in rec.calls} == {False, True}
+    assert choice.wide_solve is True and choice.team == 0
+    assert autotune.options_for(opts, choice).wide_solve is True
+    assert "FP64 solves" in choice.describe()
+
+    for fn, n, opts in ((_ring(4)[0], 8, KernelOptions(lu_precision="fp32", fast=True)),
+                        (_ring(16)[0], 32, KernelOptions(lu_precision="fp64", sparsity=_ring(16)[2])),
+                        (_ring(16)[0], 32, KernelOptions(lu_precision="fp32", fast=True, sparsity=_ring(16)[2],
+                                                         wide_solve=False))):
+        rec = Recorder(lambda c, m, s: 1.0, steps=10)
+        _tune(fn, n, opts, rec, monkeypatch)
+        assert {c.wide_solve for c, _, _ in rec.calls} == {None}

@@ -180,6 +180,39 @@ def test_gradient_config_full_horizon_within_rounding_noise(oracle, n_osc, count
                np.abs(pg - og).max(axis=1) / scale, (ap == a) & (rp == r), count)
 
 
+def test_vdp_ring_32_fp64_stage_solves_as_accurate_as_fp64(oracle):
+    """The 32-state ring's thread kernel with the stage solves in FP64 against
+    the widened FP32 factors (an autotuner candidate at this size) held to the
+    bar of the FP32-solve test below."""
+    from menodax_b200 import _native
+    from menodax_b200._ensemble import launch
+    from menodax_b200._problem import KernelOptions, get_problem, wide_solve
+
+    n_osc = 16
+    cfg, y0, mu = _ring_inputs(n_osc, 64)
+    t_span = np.linspace(0.0, 30.0, 10)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=normalize_sparsity(cfg["sparsity"], 2 * n_osc),
+                         wide_solve=True)
+    assert wide_solve(opts, 2 * n_osc)
+    problem = get_problem(cfg["ode_fn"], 2 * n_osc, 1, opts)
+    dev = torch.device("cuda", 0)
+    hist, counters = launch(problem, y0=torch.as_tensor(y0, device=dev), times=torch.as_tensor(t_span, device=dev),
+                            params=torch.as_tensor(mu, device=dev), weights=None, dt0=0.0, rtol=cfg["rtol"],
+                            atol=cfg["atol"], max_steps=100000, mode=_native.MDX_LAUNCH_PERSISTENT)
+    h32 = hist.cpu().numpy()
+    assert int(counters[3].max()) == 0
+    system = oracle.System.vdp_ring(n_osc, 1.0, 0.1)
+    ref, *_ = oracle.solve("rodas5P", system, y0, t_span, mu, rtol=1e-12, atol=1e-14, lu_precision="fp64")
+    o64, *_ = oracle.solve("rodas5P", system, y0, t_span, mu, rtol=cfg["rtol"], atol=cfg["atol"],
+                           lu_precision="fp64")
+    scale = np.abs(ref) + cfg["atol"] / cfg["rtol"]
+    err32 = (np.abs(h32 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    err64 = (np.abs(o64 - ref) / scale).reshape(len(ref), -1).max(axis=1)
+    for q in (0.5, 0.9):
+        assert np.quantile(err32, q) <= 1.5 * np.quantile(err64, q) + 10 * cfg["rtol"]
+    assert err32.max() <= 3.0 * err64.max()
+
+
 @pytest.mark.parametrize("n_osc,team", [(16, 0), (64, 8)], ids=["ring32_thread", "ring128_team8"])
 def test_vdp_ring_fp32_lu_as_accurate_as_fp64(oracle, n_osc, team):
     """Configuration 3's product path -- FP32 LU, fast arithmetic, the autotuned

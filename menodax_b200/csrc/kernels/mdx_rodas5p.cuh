@@ -32,13 +32,14 @@ typedef MDX_LU_T lu_t;
 #define MDX_AUTONOMOUS 0
 #endif
 // The triangular solves' type.  The reference solves in the LU type and rounds
-// the stage increments to it (k_stages, modax/rodas5P.py:724), and so do the
-// reference arithmetic and every large system here.  Fast arithmetic on a
-// system of up to 8 states (MDX_WIDE_SOLVE) factorises in FP32 as well but
-// solves in double against the factors, widened once per step: one conversion
-// per factor entry instead of two per component and stage, which on the B200's
-// half-rate FP64 pipe costs less than the conversions it replaces, and the
-// stages keep their full double values.
+// the stage increments to it (k_stages, modax/rodas5P.py:724), and so does the
+// reference arithmetic here.  A fast-arithmetic build with MDX_WIDE_SOLVE (the
+// host sets it for systems of up to 8 states, and for larger ones where it
+// measured faster) factorises in FP32 as well but solves in double against the
+// factors, widened once per step: one conversion per factor entry instead of
+// two per component and stage, which on the B200's half-rate FP64 pipe costs
+// less than the conversions it replaces, and the stages keep their full double
+// values.
 #ifndef MDX_SOLVE_T
 #define MDX_SOLVE_T MDX_LU_T
 #endif
@@ -47,7 +48,8 @@ typedef MDX_LU_T lu_t;
 #endif
 typedef MDX_SOLVE_T sol_t;
 // Stage increments: small systems keep them in double registers (the rounded
-// values, or the wide solve's own), larger ones in the LU type.
+// values, or the wide solve's own), larger ones in the LU type unless the
+// solve is wide.
 #if MDX_NS <= 8 || MDX_WIDE_SOLVE
 typedef double k_t;
 #else

@@ -145,6 +145,24 @@ typedef struct mdx_grad_desc {
                               which trajectories are handed to threads -- e.g. longest first by
                               ckpt_count, so the longest reverse sweeps start in the first
                               wave of resident blocks */
+  /* Split reverse (one thread per trajectory plans only; `order` and `count` are then
+   * ignored).  The reverse pass is linear in the cotangent, so a long trajectory's
+   * checkpoint segments can be cut into chunks reversed in parallel: a chunk run from
+   * the cotangent e_j at its end, with no save cotangents injected, gives column j of
+   * its transfer matrix (and the matching parameter rows); run from zero with the
+   * injections, its offset.  mdx_grad reverses every task, then composes each split
+   * trajectory's chunks last to first into grad_y0 / grad_params. */
+  const int* tasks;        /* (n_tasks, 5): trajectory, first segment, end segment, kind, slot.
+                              kind -2: the whole trajectory (segments ignored), written to
+                              grad_y0 / grad_params; -1: the chunk from zero with injections;
+                              j >= 0: the chunk from e_j without them.  Chunk tasks write
+                              (n_vars + n_params) doubles to task_out row `slot` */
+  int n_tasks;
+  int n_slots;             /* rows of task_out */
+  double* task_out;
+  const int* combine;      /* (n_combine, 3): trajectory, first slot, chunks; chunk c's task of
+                              kind k sits at slot first + c (n_vars + 1) + k + 1 */
+  int n_combine;
 } mdx_grad_desc;
 
 /* NVRTC: compile CUDA C++ `source` to an sm_100a cubin.  Needs no GPU.

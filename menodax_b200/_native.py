@@ -83,7 +83,9 @@ class GradDesc(ctypes.Structure):
         ("ckpt", ctypes.c_void_p), ("ckpt_count", ctypes.c_void_p),
         ("ckpt_capacity", ctypes.c_longlong), ("grad_hist", ctypes.c_void_p),
         ("grad_y0", ctypes.c_void_p), ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p),
-        ("order", ctypes.c_void_p),
+        ("order", ctypes.c_void_p), ("tasks", ctypes.c_void_p), ("n_tasks", ctypes.c_int),
+        ("n_slots", ctypes.c_int), ("task_out", ctypes.c_void_p), ("combine", ctypes.c_void_p),
+        ("n_combine", ctypes.c_int),
     ]
 
 
@@ -192,10 +194,12 @@ def _included_headers(source: str) -> list[str]:
 
 def compile_cubin(source: str, options: list[str], name: str = "mdx_problem.cu") -> bytes:
     """NVRTC-compile ``source`` for sm_100a, through an on-disk cache keyed on its
-    text, the text of every kernel header it includes, and the options."""
+    text, the text of every kernel header it includes, and the options.  The key
+    leaves out where the kernel headers sit on disk (their text is in it), so a
+    cache built in one checkout serves another."""
     opts = [f"-I{KERNEL_DIR}", "-arch=sm_100a", "-std=c++17", "-default-device", "-lineinfo"] + list(options)
     h = hashlib.sha256()
-    for part in (source, *opts):
+    for part in (source, "-I<kernels>", *opts[1:]):
         h.update(part.encode())
         h.update(b"\0")
     for header in _included_headers(source):

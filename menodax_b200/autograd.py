@@ -108,6 +108,51 @@ def reverse_chunk(problem, n: int) -> int:
     return max(1, min(n, REVERSE_CHUNK or n))
 
 
+# The reverse sweep of a trajectory with more than REVERSE_SPLIT times the mean
+# number of checkpoint segments is cut into chunks of at most that many, reversed
+# in parallel and composed (None: never).  A gradient's reverse pass is set by its
+# longest trajectories; a chunk costs n_vars + 1 sweeps (its transfer matrix's
+# columns and its offset), so only the tail is worth cutting.
+REVERSE_SPLIT: float | None = 2.0
+
+
+def split_plan(counts, capacity: int, stride: int, n_vars: int, factor: float | None = None):
+    """The split reverse's task table for trajectories with ``counts`` accepted
+    steps (a CPU int tensor): ``(tasks, n_slots, combine)`` as int32 tensors
+    (``mdx_grad_desc.tasks`` / ``combine``), longest tasks first, or ``None`` when
+    no trajectory is long enough to split."""
+    import numpy as np
+
+    factor = REVERSE_SPLIT if factor is None else factor
+    steps = np.minimum(counts.numpy().astype(np.int64), int(capacity))
+    n = steps.shape[0]
+    if factor is None or n == 0:
+        return None
+    n_seg = (steps + stride - 1) // stride
+    limit = max(1, int(np.ceil(factor * float(n_seg.mean()))))
+    long_traj = np.nonzero(n_seg > limit)[0]
+    if long_traj.size == 0:
+        return None
+    short = np.nonzero(n_seg <= limit)[0]
+    rows = [np.stack([n_seg[short], short, np.zeros_like(short), n_seg[short],
+                      np.full_like(short, -2), np.full_like(short, -1)], axis=1)]
+    combine = []
+    slot = 0
+    for traj in long_traj:
+        total = int(n_seg[traj])
+        chunks = -(-total // limit)
+        combine.append((int(traj), slot, chunks))
+        for c in range(chunks):
+            lo, hi = c * total // chunks, (c + 1) * total // chunks
+            for kind in range(-1, n_vars):
+                rows.append(np.array([[hi - lo, traj, lo, hi, kind, slot]], dtype=np.int64))
+                slot += 1
+    table = np.concatenate(rows, axis=0)
+    table = table[np.argsort(-table[:, 0], kind="stable")]
+    tasks = torch.as_tensor(table[:, 1:].astype(np.int32))
+    return tasks, slot, torch.as_tensor(np.asarray(combine, dtype=np.int32))
+
+
 class _EnsembleSolve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, y0, params, times, problems, dt0, rtol, atol, max_steps, key):
@@ -168,11 +213,28 @@ class _EnsembleSolve(torch.autograd.Function):
         d.grad_y0 = grad_y0.data_ptr()
         d.grad_params = grad_p.data_ptr()
         d.status = status.data_ptr()
+        stream = torch.cuda.current_stream(params.device).cuda_stream
+        plan = None
+        if not problem.options.team and REVERSE_CHUNK is None:
+            plan = split_plan(ckpt_count.cpu(), ctx.capacity, int(problem.options.ckpt_stride), problem.n_vars)
+        if plan is not None:
+            tasks, n_slots, combine = plan
+            tasks = tasks.to(params.device)
+            combine = combine.to(params.device)
+            task_out = torch.empty((max(1, n_slots), problem.n_vars + problem.n_params), dtype=torch.float64,
+                                   device=params.device)
+            d.tasks, d.n_tasks = tasks.data_ptr(), tasks.shape[0]
+            d.task_out, d.n_slots = task_out.data_ptr(), n_slots
+            d.combine, d.n_combine = combine.data_ptr(), combine.shape[0]
+            last_checkpoint.update(split_tasks=int(tasks.shape[0]), split_trajectories=int(combine.shape[0]))
+            with torch.cuda.device(params.device):
+                problem.plan.grad(d, stream)
+            return grad_y0, grad_p, None, None, None, None, None, None, None
+        last_checkpoint.update(split_tasks=0, split_trajectories=0)
         # Longest reverse sweeps first: the reverse kernel's registers leave room
         # for only part of a large ensemble at once, and a long trajectory that
         # started in a later wave would set the makespan.
         order = torch.argsort(ckpt_count, descending=True, stable=True).to(torch.int32)
-        stream = torch.cuda.current_stream(params.device).cuda_stream
         chunk = reverse_chunk(problem, n)
         with torch.cuda.device(params.device):
             for first in range(0, n, chunk):

@@ -372,38 +372,28 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 // recorded step sizes) to recover every step's start state, then reversed step
 // by step.  Saves after the last accepted step hold the final state (Rodas5P's
 // frozen saves); save 0 is y0 itself.
-extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
-mdx_grad_reverse(const MdxGradArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n_run) return;
-  const int traj = a.order ? a.order[i] : i;
-  double p[MDX_NP > 0 ? MDX_NP : 1];
-#pragma unroll
-  for (int k = 0; k < MDX_NP; ++k) p[k] = a.params[(size_t)traj * MDX_NP + k];
-  double pbar[MDX_NP > 0 ? MDX_NP : 1];
-#pragma unroll
-  for (int k = 0; k < MDX_NP; ++k) pbar[k] = 0.0;
-  double ybar[MDX_NV];
-#pragma unroll
-  for (int j = 0; j < MDX_NV; ++j) ybar[j] = 0.0;
-  const int n_steps = a.ckpt_count[traj];
-  int status = 0;
-  if (n_steps > a.ckpt_capacity) status |= MDX_STATUS_CKPT_OVERFLOW;
-  const int steps = n_steps < a.ckpt_capacity ? n_steps : (int)a.ckpt_capacity;
-  int s_hi = 0;
-  if (steps == 0) {
-    for (int sv = 1; sv < a.n_save; ++sv) {
-      const double* g = mdx::adjoint::grad_row(a, traj, sv);
-#pragma unroll
-      for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
-    }
-  }
+//
+// reverse_segments reverses segments [seg_lo, seg_hi) of one trajectory with
+// `steps` recorded steps, ybar holding the cotangent at the end of segment
+// seg_hi - 1 on entry and at the start of segment seg_lo on exit; pbar
+// accumulates.  With `inject` the saves' cotangents (grad_hist) inside the range
+// are added as their steps are reversed, and, when the range ends with the last
+// step, those of the frozen saves first; without it the pass is the homogeneous
+// linear map, which a split trajectory's chunks are composed from.
+namespace mdx {
+namespace adjoint {
+
+__device__ __forceinline__ void reverse_segments(const MdxGradArgs& a, int traj, const double* p, int steps,
+                                                 int seg_lo, int seg_hi, bool inject,
+                                                 double (&ybar)[MDX_NV],
+                                                 double (&pbar)[MDX_NP > 0 ? MDX_NP : 1]) {
   double yseg[MDX_CKPT_SEG][MDX_NV];
   double tseg[MDX_CKPT_SEG];
-  for (int seg = (steps - 1) / MDX_CKPT_SEG; steps > 0 && seg >= 0; --seg) {
+  int s_hi = 0;
+  for (int seg = seg_hi - 1; seg >= seg_lo; --seg) {
     const int m0 = seg * MDX_CKPT_SEG;
     const int m1 = (m0 + MDX_CKPT_SEG < steps) ? m0 + MDX_CKPT_SEG : steps;
-    const double* rec = mdx::adjoint::ckpt_seg_state(a, seg, traj);
+    const double* rec = ckpt_seg_state(a, seg, traj);
     double y[MDX_NV];
     double t = rec[0];
 #pragma unroll
@@ -412,39 +402,149 @@ mdx_grad_reverse(const MdxGradArgs a) {
       tseg[m - m0] = t;
 #pragma unroll
       for (int j = 0; j < MDX_NV; ++j) yseg[m - m0][j] = y[j];
-      const double h = mdx::adjoint::ckpt_h(a, m, traj);
+      const double h = ckpt_h(a, m, traj);
       if (m + 1 < m1) {
         double y_next[MDX_NV];
-        mdx::adjoint::replay_step(t, h, y, p, y_next);
+        replay_step(t, h, y, p, y_next);
 #pragma unroll
         for (int j = 0; j < MDX_NV; ++j) y[j] = y_next[j];
       }
       t += h;
     }
-    if (m1 == steps) {
-      // t is now the end time of the last accepted step: later saves are frozen.
-      s_hi = mdx::adjoint::last_save_reached(a.times, a.n_save - 1, t);
-      for (int sv = s_hi + 1; sv < a.n_save; ++sv) {
-        const double* g = mdx::adjoint::grad_row(a, traj, sv);
+    if (seg == seg_hi - 1) {
+      // t is now the end time of the range's last step: the saves it reached
+      // are the ones its steps own.
+      s_hi = last_save_reached(a.times, a.n_save - 1, t);
+      if (inject && m1 == steps) {
+        // Later saves are frozen at the final state.
+        for (int sv = s_hi + 1; sv < a.n_save; ++sv) {
+          const double* g = grad_row(a, traj, sv);
 #pragma unroll
-        for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+          for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+        }
       }
     }
     for (int m = m1 - 1; m >= m0; --m) {
       const double tm = tseg[m - m0];
-      const double h = mdx::adjoint::ckpt_h(a, m, traj);
+      const double h = ckpt_h(a, m, traj);
       double ym[MDX_NV];
 #pragma unroll
       for (int j = 0; j < MDX_NV; ++j) ym[j] = yseg[m - m0][j];
-      const int s_lo = m == 0 ? 0 : mdx::adjoint::last_save_reached(a.times, s_hi, tm);
-      mdx::adjoint::reverse_step(a, traj, tm, h, ym, p, s_lo, s_hi, ybar, pbar);
+      const int s_lo = m == 0 ? 0 : last_save_reached(a.times, s_hi, tm);
+      reverse_step(a, traj, tm, h, ym, p, inject ? s_lo : s_hi, s_hi, ybar, pbar);
       s_hi = s_lo;
     }
   }
-  const double* g0 = mdx::adjoint::grad_row(a, traj, 0);
+}
+
+}  // namespace adjoint
+}  // namespace mdx
+
+extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
+mdx_grad_reverse(const MdxGradArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_run) return;
+  int traj, seg_lo = 0, seg_hi = 0, kind = -2, slot = -1;
+  if (a.tasks) {
+    const int* task = a.tasks + (size_t)i * 5;
+    traj = task[0];
+    seg_lo = task[1];
+    seg_hi = task[2];
+    kind = task[3];
+    slot = task[4];
+  } else {
+    traj = a.order ? a.order[i] : i;
+  }
+  if (traj < 0 || traj >= a.n_traj || kind < -2 || kind >= MDX_NV) return;
+  double p[MDX_NP > 0 ? MDX_NP : 1];
 #pragma unroll
-  for (int j = 0; j < MDX_NV; ++j) a.grad_y0[(size_t)traj * MDX_NV + j] = ybar[j] + g0[j];
+  for (int k = 0; k < MDX_NP; ++k) p[k] = a.params[(size_t)traj * MDX_NP + k];
+  double pbar[MDX_NP > 0 ? MDX_NP : 1];
 #pragma unroll
-  for (int k = 0; k < MDX_NP; ++k) a.grad_params[(size_t)traj * MDX_NP + k] = pbar[k];
-  if (a.status) a.status[traj] = status;
+  for (int k = 0; k < MDX_NP; ++k) pbar[k] = 0.0;
+  double ybar[MDX_NV];
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) ybar[j] = kind == j ? 1.0 : 0.0;
+  const int n_steps = a.ckpt_count[traj];
+  const int steps = n_steps < a.ckpt_capacity ? n_steps : (int)a.ckpt_capacity;
+  const int n_seg = (steps + MDX_CKPT_SEG - 1) / MDX_CKPT_SEG;
+  if (kind == -2) {
+    seg_lo = 0;
+    seg_hi = n_seg;
+  } else if (seg_lo < 0 || seg_hi > n_seg || seg_lo >= seg_hi || slot < 0 || slot >= a.n_slots) {
+    return;
+  }
+  const bool inject = kind < 0;
+  if (steps == 0 && inject) {
+    for (int sv = 1; sv < a.n_save; ++sv) {
+      const double* g = mdx::adjoint::grad_row(a, traj, sv);
+#pragma unroll
+      for (int j = 0; j < MDX_NV; ++j) ybar[j] += g[j];
+    }
+  }
+  mdx::adjoint::reverse_segments(a, traj, p, steps, seg_lo, seg_hi, inject, ybar, pbar);
+  if (inject && seg_lo == 0) {
+    const double* g0 = mdx::adjoint::grad_row(a, traj, 0);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) ybar[j] += g0[j];
+  }
+  if (kind == -2) {
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) a.grad_y0[(size_t)traj * MDX_NV + j] = ybar[j];
+#pragma unroll
+    for (int k = 0; k < MDX_NP; ++k) a.grad_params[(size_t)traj * MDX_NP + k] = pbar[k];
+    if (a.status) a.status[traj] = n_steps > a.ckpt_capacity ? MDX_STATUS_CKPT_OVERFLOW : 0;
+  } else {
+    double* out = a.task_out + (size_t)slot * (MDX_NV + MDX_NP);
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) out[j] = ybar[j];
+#pragma unroll
+    for (int k = 0; k < MDX_NP; ++k) out[MDX_NV + k] = pbar[k];
+  }
+}
+
+// Composes each split trajectory's chunks, last to first: with the cotangent
+// lambda at a chunk's end, its start gets A lambda + b and the parameters
+// P lambda + q, where column j of [A; P] is the chunk's unit task j and [b; q]
+// its injecting task.
+extern "C" __global__ void __launch_bounds__(MDX_TPB, MDX_MIN_BLOCKS)
+mdx_grad_combine(const MdxGradArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n_combine) return;
+  const int traj = a.combine[(size_t)k * 3];
+  const int first = a.combine[(size_t)k * 3 + 1];
+  const int chunks = a.combine[(size_t)k * 3 + 2];
+  constexpr int W = MDX_NV + MDX_NP;
+  constexpr int PER_CHUNK = MDX_NV + 1;
+  if (traj < 0 || traj >= a.n_traj || chunks < 1 || first < 0 || first + chunks * PER_CHUNK > a.n_slots) return;
+  double lam[MDX_NV];
+  double pb[MDX_NP > 0 ? MDX_NP : 1];
+  const double* last = a.task_out + (size_t)(first + (chunks - 1) * PER_CHUNK) * W;
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) lam[j] = last[j];
+#pragma unroll
+  for (int q = 0; q < MDX_NP; ++q) pb[q] = last[MDX_NV + q];
+  for (int c = chunks - 2; c >= 0; --c) {
+    const double* base = a.task_out + (size_t)(first + c * PER_CHUNK) * W;
+    double next[MDX_NV];
+#pragma unroll
+    for (int i = 0; i < MDX_NV; ++i) next[i] = base[i];
+#pragma unroll
+    for (int q = 0; q < MDX_NP; ++q) pb[q] += base[MDX_NV + q];
+#pragma unroll
+    for (int j = 0; j < MDX_NV; ++j) {
+      const double* col = base + (size_t)(j + 1) * W;
+#pragma unroll
+      for (int i = 0; i < MDX_NV; ++i) next[i] += col[i] * lam[j];
+#pragma unroll
+      for (int q = 0; q < MDX_NP; ++q) pb[q] += col[MDX_NV + q] * lam[j];
+    }
+#pragma unroll
+    for (int i = 0; i < MDX_NV; ++i) lam[i] = next[i];
+  }
+#pragma unroll
+  for (int j = 0; j < MDX_NV; ++j) a.grad_y0[(size_t)traj * MDX_NV + j] = lam[j];
+#pragma unroll
+  for (int q = 0; q < MDX_NP; ++q) a.grad_params[(size_t)traj * MDX_NP + q] = pb[q];
+  if (a.status) a.status[traj] = a.ckpt_count[traj] > a.ckpt_capacity ? MDX_STATUS_CKPT_OVERFLOW : 0;
 }

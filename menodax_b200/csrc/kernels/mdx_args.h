@@ -55,7 +55,12 @@ typedef struct MdxGradArgs {
   long long ckpt_capacity;
   int n_traj;              /* trajectories in the buffers (their stride) */
   int n_save;
-  int n_run;               /* threads of this launch: order[0..n_run) */
+  int n_run;               /* threads of this launch: order[0..n_run), or tasks[0..n_run) */
+  const int* tasks;        /* split reverse: (n_run, 5) traj, first segment, end segment, kind, slot */
+  double* task_out;        /* (n_slots, n_vars + n_params) */
+  const int* combine;      /* (n_combine, 3) traj, first slot, chunks */
+  int n_slots;
+  int n_combine;
 } MdxGradArgs;
 
 #endif

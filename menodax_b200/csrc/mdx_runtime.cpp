@@ -162,6 +162,7 @@ struct Loaded {
   CUfunction plain = nullptr;
   CUfunction persistent = nullptr;
   CUfunction grad = nullptr;
+  CUfunction combine = nullptr;  // thread adjoint modules: the split reverse's composition
   int sm_count = 0;
 };
 
@@ -213,6 +214,9 @@ int load_for_context(mdx_plan* plan, Loaded** out) {
   if (plan->desc.flags & MDX_PLAN_ADJOINT) {
     if ((r = g_driver.moduleGetFunction(&l.grad, guard.module, "mdx_grad_reverse")) != CUDA_SUCCESS)
       return cuda_fail(r, "cuModuleGetFunction(mdx_grad_reverse)");
+    if (plan->desc.team_size == 1 &&
+        (r = g_driver.moduleGetFunction(&l.combine, guard.module, "mdx_grad_combine")) != CUDA_SUCCESS)
+      return cuda_fail(r, "cuModuleGetFunction(mdx_grad_combine)");
   }
   // Above the 48 KB default a kernel's dynamic shared memory has to be opted into.
   if (plan->desc.shared_bytes > 48 * 1024) {
@@ -563,6 +567,18 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
   if (d->n_traj < 0 || d->n_save < 1) return fail(MDX_E_INVALID, "bad sizes n_traj=%d n_save=%d", d->n_traj, d->n_save);
   if (d->count < 0 || d->count > d->n_traj)
     return fail(MDX_E_INVALID, "mdx_grad: count %d outside [0, n_traj = %d]", d->count, d->n_traj);
+  const bool split = d->tasks != nullptr;
+  if (split) {
+    if (plan->desc.team_size != 1)
+      return fail(MDX_E_INVALID, "mdx_grad: the split reverse needs a one-thread-per-trajectory plan");
+    if (d->n_tasks < 0 || d->n_slots < 0 || d->n_combine < 0 || (d->n_slots > 0 && !d->task_out) ||
+        (d->n_combine > 0 && !d->combine))
+      return fail(MDX_E_INVALID, "mdx_grad: split reverse needs n_tasks, n_slots, n_combine >= 0 and "
+                  "task_out / combine when slots / combinations are used");
+    if (d->n_combine > 0 && d->n_combine * (plan->desc.n_vars + 1) > d->n_slots)
+      return fail(MDX_E_INVALID, "mdx_grad: %d combinations need at least %d slots; got %d", d->n_combine,
+                  d->n_combine * (plan->desc.n_vars + 1), d->n_slots);
+  }
   if (d->n_traj == 0) return MDX_OK;
   if (!d->times || !d->ckpt || !d->ckpt_count || !d->grad_hist || !d->grad_y0 || !d->grad_params ||
       d->ckpt_capacity < 1)
@@ -585,13 +601,30 @@ int mdx_grad(mdx_plan* plan, const mdx_grad_desc* d, void* stream) {
   a.n_traj = d->n_traj;
   a.n_save = d->n_save;
   a.n_run = d->count > 0 ? d->count : d->n_traj;
+  if (split) {
+    a.order = nullptr;
+    a.tasks = d->tasks;
+    a.task_out = d->task_out;
+    a.combine = d->combine;
+    a.n_slots = d->n_slots;
+    a.n_combine = d->n_combine;
+    a.n_run = d->n_tasks;
+  }
   const unsigned tpb = (unsigned)plan->desc.threads_per_block;
   // Trajectories per block: one per thread, or one per team of team_size lanes.
   const unsigned per_block = tpb / (unsigned)plan->desc.team_size;
-  const unsigned grid = (unsigned)((a.n_run + per_block - 1) / per_block);
   void* params[] = {&a};
-  CUresult r = g_driver.launchKernel(l->grad, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
-  if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_reverse)");
+  CUresult r;
+  if (a.n_run > 0) {
+    const unsigned grid = (unsigned)((a.n_run + per_block - 1) / per_block);
+    r = g_driver.launchKernel(l->grad, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
+    if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_reverse)");
+  }
+  if (split && a.n_combine > 0) {
+    const unsigned grid = (unsigned)((a.n_combine + tpb - 1) / tpb);
+    r = g_driver.launchKernel(l->combine, grid, 1, 1, tpb, 1, 1, 0, (CUstream)stream, params, nullptr);
+    if (r != CUDA_SUCCESS) return cuda_fail(r, "cuLaunchKernel(mdx_grad_combine)");
+  }
   return MDX_OK;
 }
 

@@ -306,3 +306,36 @@ def test_team_adjoint_matches_the_thread_adjoint(n_osc):
     for got, ref in ((gy8, gy0), (gp8, gp0)):
         scale = np.abs(ref).max(axis=1, keepdims=True) + 1e-300
         assert (np.abs(got - ref) / scale).max() < 1e-7
+
+
+@pytest.mark.parametrize("solve,n_osc,kw", [
+    (rodas5P.solve, 1, dict(lu_precision="fp64")),
+    (rodas5P.solve, 3, dict(lu_precision="fp32", sparsity=systems.vdp_sparsity(3))),
+    (tsit5.solve, None, {}),
+], ids=["vdp2_fp64", "ring6_fp32_sparse", "lorenz_tsit5"])
+def test_split_reverse_gives_the_whole_reverse(monkeypatch, solve, n_osc, kw):
+    """The reverse pass with long trajectories cut into chunks (transfer matrices
+    from unit cotangents, offsets from the injected ones, composed afterwards)
+    equals the one-sweep-per-trajectory reverse to rounding; cut at half the mean
+    length, most trajectories are split."""
+    from menodax_b200 import autograd
+
+    if n_osc is None:
+        cfg = systems.lorenz_config(size=512)
+        t_span, fn, y0, p = cfg["t_span"], cfg["ode_fn"], cfg["y0"], cfg["params"]
+        kw = dict(kw, rtol=cfg["rtol"], atol=cfg["atol"])
+    else:
+        cfg = systems.vdp_gradient_config(n_osc, size=512)
+        t_span, fn, y0, p = np.linspace(0.0, 50.0, 11), cfg["ode_fn"], cfg["y0"], cfg["params"]
+        kw = dict(kw, rtol=cfg["rtol"], atol=cfg["atol"])
+    w = np.random.default_rng(13).normal(size=(512, len(t_span), y0.shape[1]))
+    monkeypatch.setattr(autograd, "REVERSE_SPLIT", None)
+    h0, gy0, gp0 = _grads(solve, fn, y0, t_span, p, w, **kw)
+    assert autograd.last_checkpoint["split_tasks"] == 0
+    monkeypatch.setattr(autograd, "REVERSE_SPLIT", 0.5)
+    h1, gy1, gp1 = _grads(solve, fn, y0, t_span, p, w, **kw)
+    assert autograd.last_checkpoint["split_trajectories"] > 100
+    assert np.array_equal(h0, h1)
+    for a, b in ((gy0, gy1), (gp0, gp1)):
+        scale = np.abs(a).max(axis=1, keepdims=True) + 1e-300
+        assert (np.abs(a - b) / scale).max() < 1e-9

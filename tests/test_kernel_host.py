@@ -214,6 +214,11 @@ extern "C" void run_grad(MdxGradArgs g) {
   blockIdx.x = 0; blockDim.x = 1;
   for (int i = 0; i < g.n_traj; ++i) { threadIdx.x = (unsigned)i; mdx_grad_reverse(g); }
 }
+extern "C" void run_grad_tasks(MdxGradArgs g) {
+  blockIdx.x = 0; blockDim.x = 1;
+  for (int i = 0; i < g.n_run; ++i) { threadIdx.x = (unsigned)i; mdx_grad_reverse(g); }
+  for (int k = 0; k < g.n_combine; ++k) { threadIdx.x = (unsigned)k; mdx_grad_combine(g); }
+}
 """
 
 
@@ -224,7 +229,8 @@ class GradArgs(ctypes.Structure):
                 ("ckpt_count", ctypes.c_void_p), ("grad_hist", ctypes.c_void_p), ("grad_y0", ctypes.c_void_p),
                 ("grad_params", ctypes.c_void_p), ("status", ctypes.c_void_p), ("order", ctypes.c_void_p),
                 ("ckpt_capacity", ctypes.c_longlong), ("n_traj", ctypes.c_int), ("n_save", ctypes.c_int),
-                ("n_run", ctypes.c_int)]
+                ("n_run", ctypes.c_int), ("tasks", ctypes.c_void_p), ("task_out", ctypes.c_void_p),
+                ("combine", ctypes.c_void_p), ("n_slots", ctypes.c_int), ("n_combine", ctypes.c_int)]
 
 
 def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
@@ -242,10 +248,11 @@ def _host_adjoint(tmp_path, name, fn, n_vars, n_params, options):
     lib.run.argtypes = [Args]
     lib.run.restype = ctypes.c_int
     lib.run_grad.argtypes = [GradArgs]
+    lib.run_grad_tasks.argtypes = [GradArgs]
     return lib
 
 
-def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity):
+def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity, split=None):
     """Checkpointing forward pass, then the reverse sweep of sum(w * hist)."""
     y0 = np.ascontiguousarray(y0, dtype=np.float64)
     times = np.ascontiguousarray(times, dtype=np.float64)
@@ -276,7 +283,24 @@ def _value_and_grad(lib, y0, times, params, w, rtol, atol, stride, capacity):
     g.grad_hist, g.grad_y0, g.grad_params, g.status = w.ctypes.data, grad_y0.ctypes.data, grad_p.ctypes.data, \
         status.ctypes.data
     g.ckpt_capacity, g.n_traj, g.n_save, g.n_run = capacity, n, len(times), n
-    lib.run_grad(g)
+    if split is None:
+        lib.run_grad(g)
+    else:
+        # The split reverse's task table from autograd.split_plan at factor `split`.
+        import torch
+
+        from menodax_b200.autograd import split_plan
+
+        plan = split_plan(torch.as_tensor(ckpt_count), capacity, stride, n_vars, factor=split)
+        assert plan is not None
+        tasks, n_slots, combine = (x.numpy() if hasattr(x, "numpy") else x for x in plan)
+        tasks = np.ascontiguousarray(tasks, dtype=np.int32)
+        combine = np.ascontiguousarray(combine, dtype=np.int32)
+        task_out = np.full((n_slots, n_vars + params.shape[1]), np.nan)
+        g.tasks, g.task_out, g.combine = tasks.ctypes.data, task_out.ctypes.data, combine.ctypes.data
+        g.n_run, g.n_slots, g.n_combine = tasks.shape[0], n_slots, combine.shape[0]
+        lib.run_grad_tasks(g)
+        assert not np.isnan(task_out).any()
     assert (status == 0).all()
     return hist, grad_y0, grad_p
 
@@ -345,6 +369,36 @@ def test_wide_solve_adjoint_replays_the_forward_steps_exactly(tmp_path, layout):
     for a, b in zip(out[1][1:], out[8][1:]):
         assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
     assert np.abs(out[1][1]).max() > 0.0
+
+
+@pytest.mark.parametrize("solver,stride", [("rodas5P", 1), ("rodas5P", 8), ("tsit5", 8)])
+def test_split_reverse_composes_to_the_whole_reverse(tmp_path, solver, stride):
+    """Long trajectories' reverse sweeps cut into chunks (each chunk's transfer
+    matrix from unit cotangents, its offset from the injected save cotangents),
+    reversed independently and composed, give the gradient of the whole sweep to
+    rounding; cut at half the mean segment count, nearly every trajectory is split
+    into several chunks."""
+    if solver == "rodas5P":
+        n_osc = 3
+        cfg = systems.vdp_gradient_config(n_osc, size=16)
+        fn, n_vars, n_params = cfg["ode_fn"], 2 * n_osc, 1
+        options = KernelOptions(lu_precision="fp64", checkpoint=True, adjoint=True, ckpt_stride=stride,
+                                sparsity=normalize_sparsity(systems.vdp_sparsity(n_osc), 2 * n_osc))
+        t_span, rtol, atol = np.linspace(0.0, 5.0, 6), 1e-8, 1e-10
+    else:
+        cfg = systems.lorenz_config(size=16)
+        fn, n_vars, n_params = cfg["ode_fn"], 3, 1
+        options = KernelOptions(solver="tsit5", checkpoint=True, adjoint=True, ckpt_stride=stride)
+        t_span, rtol, atol = cfg["t_span"], cfg["rtol"], cfg["atol"]
+    lib = _host_adjoint(tmp_path, f"split_{solver}_{stride}", fn, n_vars, n_params, options)
+    w = np.random.default_rng(21).normal(size=(16, len(t_span), n_vars))
+    whole = _value_and_grad(lib, cfg["y0"], t_span, cfg["params"], w, rtol, atol, stride, capacity=4096)
+    split = _value_and_grad(lib, cfg["y0"], t_span, cfg["params"], w, rtol, atol, stride, capacity=4096,
+                            split=0.5)
+    assert np.array_equal(whole[0], split[0])
+    for a, b in zip(whole[1:], split[1:]):
+        scale = np.abs(a).max(axis=1, keepdims=True) + 1e-300
+        assert (np.abs(a - b) / scale).max() < 1e-9
 
 
 def test_rodas5p_time_derivative_and_tf_index(tmp_path):

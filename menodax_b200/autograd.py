@@ -110,10 +110,12 @@ def reverse_chunk(problem, n: int) -> int:
 
 # The reverse sweep of a trajectory with more than REVERSE_SPLIT times the mean
 # number of checkpoint segments is cut into chunks of at most that many, reversed
-# in parallel and composed (None: never).  A gradient's reverse pass is set by its
-# longest trajectories; a chunk costs n_vars + 1 sweeps (its transfer matrix's
-# columns and its offset), so only the tail is worth cutting.
-REVERSE_SPLIT: float | None = 2.0
+# in parallel and composed (None: never, the default).  A chunk costs n_vars + 1
+# sweeps (its transfer matrix's columns and its offset), so splitting pays only
+# when a few trajectories are far longer than the rest; on config 5's ensembles
+# the long trajectories are a sizeable fraction (at 2.5 x the mean, 5,141 of
+# 65,536 2-state trajectories), and splitting them made the reverse pass slower.
+REVERSE_SPLIT: float | None = None
 
 
 def split_plan(counts, capacity: int, stride: int, n_vars: int, factor: float | None = None):

@@ -42,6 +42,11 @@ from menodax_b200._problem import get_problem
 # Checkpoint capacity (accepted steps per trajectory) and stride last used per
 # problem, so a repeated gradient call sizes its buffer without a counting pass.
 _capacity_hint: dict = {}
+# Per problem key: the trajectories of the last call, longest first (by accepted
+# steps).  The checkpointing forward launch takes them in that order, so the
+# long integrations start in the persistent grid's first wave; results do not
+# depend on the order.
+_order_hint: dict = {}
 # The checkpoint layout of the most recent gradient forward pass (for reports).
 last_checkpoint: dict = {}
 
@@ -83,6 +88,12 @@ def _as_double(x, device):
     if isinstance(x, torch.Tensor):
         return x.to(device=device, dtype=torch.float64)
     return torch.as_tensor(x, dtype=torch.float64, device=device)
+
+
+def _longest_first(accepted):
+    """Trajectory indices by descending step count, as the int32 visiting order
+    the persistent launch takes."""
+    return torch.argsort(accepted, descending=True, stable=True).to(torch.int32)
 
 
 def _half_fill(problem, n: int) -> int:
@@ -164,10 +175,14 @@ class _EnsembleSolve(torch.autograd.Function):
         kw = dict(y0=y0c, times=times, params=pc, weights=None, dt0=dt0, rtol=rtol, atol=atol,
                   max_steps=max_steps, mode=_native.MDX_LAUNCH_PERSISTENT)
         capacity, stride_hint = _capacity_hint.get(key, (None, None))
+        order = _order_hint.get(key)
+        if order is not None and (order.device != y0.device or order.numel() != n):
+            order = None
         if capacity is None:
             # First call for this problem: count the accepted steps with a plain solve.
             _, counters = launch(problems["plain"], grid_blocks=_half_fill(problems["plain"], n), **kw)
             capacity = max(1, int(counters[0].max().item()) if n else 1)
+            order = _longest_first(counters[0])
         while True:
             stride = choose_stride(n, problems["plain"].n_vars, capacity, y0.device)
             # Keep the last call's stride when memory still allows it: the same
@@ -179,13 +194,14 @@ class _EnsembleSolve(torch.autograd.Function):
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
             hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity,
-                                    grid_blocks=_half_fill(problem, n), **kw)
+                                    grid_blocks=_half_fill(problem, n), order=order, **kw)
             needed = int(counters[0].max().item()) if n else 0
             if needed <= capacity:
                 break
             capacity = int(needed * 1.1) + 8
             del ckpt
         _capacity_hint[key] = (max(needed + 8, int(needed * 1.1)), stride)
+        _order_hint[key] = _longest_first(counters[0])
         last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes)
         ctx.problem = problem
         ctx.capacity = capacity

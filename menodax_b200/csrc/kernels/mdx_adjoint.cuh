@@ -383,6 +383,44 @@ __device__ __forceinline__ void reverse_step(const MdxGradArgs& a, int traj, dou
 namespace mdx {
 namespace adjoint {
 
+// Small systems load the segment below's start record and step sizes while the
+// current segment is being reversed: a sweep that has the SM to itself (the
+// longest trajectories, last) would otherwise wait on each segment's loads.
+#define MDX_SEG_PREFETCH (MDX_NV <= 8 && MDX_CKPT_SEG <= 8)
+
+struct SegmentData {
+  double rec[MDX_NV + 1];  // t, y at the segment's first step
+  double h[MDX_SEG_PREFETCH ? MDX_CKPT_SEG : 1];
+};
+
+__device__ __forceinline__ void load_segment(const MdxGradArgs& a, int seg, int traj, int steps, SegmentData& d) {
+  const double* rec = ckpt_seg_state(a, seg, traj);
+#pragma unroll
+  for (int j = 0; j <= MDX_NV; ++j) d.rec[j] = __ldg(rec + j);
+#if MDX_SEG_PREFETCH
+  const int m0 = seg * MDX_CKPT_SEG;
+#pragma unroll
+  for (int k = 0; k < MDX_CKPT_SEG; ++k)
+    if (m0 + k < steps) d.h[k] = __ldg(a.ckpt + (size_t)(m0 + k) * (size_t)a.n_traj + (size_t)traj);
+#endif
+}
+
+__device__ __forceinline__ double segment_h(const MdxGradArgs& a, const SegmentData& d, int m, int m0, int traj) {
+#if MDX_SEG_PREFETCH
+  (void)a;
+  (void)traj;
+  double h = d.h[0];
+#pragma unroll
+  for (int k = 1; k < MDX_CKPT_SEG; ++k)
+    if (m - m0 == k) h = d.h[k];
+  return h;
+#else
+  (void)d;
+  (void)m0;
+  return ckpt_h(a, m, traj);
+#endif
+}
+
 __device__ __forceinline__ void reverse_segments(const MdxGradArgs& a, int traj, const double* p, int steps,
                                                  int seg_lo, int seg_hi, bool inject,
                                                  double (&ybar)[MDX_NV],
@@ -390,19 +428,24 @@ __device__ __forceinline__ void reverse_segments(const MdxGradArgs& a, int traj,
   double yseg[MDX_CKPT_SEG][MDX_NV];
   double tseg[MDX_CKPT_SEG];
   int s_hi = 0;
+  SegmentData cur;
+  if (seg_hi > seg_lo) load_segment(a, seg_hi - 1, traj, steps, cur);
   for (int seg = seg_hi - 1; seg >= seg_lo; --seg) {
     const int m0 = seg * MDX_CKPT_SEG;
     const int m1 = (m0 + MDX_CKPT_SEG < steps) ? m0 + MDX_CKPT_SEG : steps;
-    const double* rec = ckpt_seg_state(a, seg, traj);
+    SegmentData next;
+#if MDX_SEG_PREFETCH
+    if (seg > seg_lo) load_segment(a, seg - 1, traj, steps, next);
+#endif
     double y[MDX_NV];
-    double t = rec[0];
+    double t = cur.rec[0];
 #pragma unroll
-    for (int j = 0; j < MDX_NV; ++j) y[j] = rec[1 + j];
+    for (int j = 0; j < MDX_NV; ++j) y[j] = cur.rec[1 + j];
     for (int m = m0; m < m1; ++m) {
       tseg[m - m0] = t;
 #pragma unroll
       for (int j = 0; j < MDX_NV; ++j) yseg[m - m0][j] = y[j];
-      const double h = ckpt_h(a, m, traj);
+      const double h = segment_h(a, cur, m, m0, traj);
       if (m + 1 < m1) {
         double y_next[MDX_NV];
         replay_step(t, h, y, p, y_next);
@@ -426,13 +469,20 @@ __device__ __forceinline__ void reverse_segments(const MdxGradArgs& a, int traj,
     }
     for (int m = m1 - 1; m >= m0; --m) {
       const double tm = tseg[m - m0];
-      const double h = ckpt_h(a, m, traj);
+      const double h = segment_h(a, cur, m, m0, traj);
       double ym[MDX_NV];
 #pragma unroll
       for (int j = 0; j < MDX_NV; ++j) ym[j] = yseg[m - m0][j];
       const int s_lo = m == 0 ? 0 : last_save_reached(a.times, s_hi, tm);
       reverse_step(a, traj, tm, h, ym, p, inject ? s_lo : s_hi, s_hi, ybar, pbar);
       s_hi = s_lo;
+    }
+    if (seg > seg_lo) {
+#if MDX_SEG_PREFETCH
+      cur = next;
+#else
+      load_segment(a, seg - 1, traj, steps, cur);
+#endif
     }
   }
 }

@@ -339,3 +339,23 @@ def test_split_reverse_gives_the_whole_reverse(monkeypatch, solve, n_osc, kw):
     for a, b in ((gy0, gy1), (gp0, gp1)):
         scale = np.abs(a).max(axis=1, keepdims=True) + 1e-300
         assert (np.abs(a - b) / scale).max() < 1e-9
+
+
+def test_forward_visiting_order_changes_nothing_but_the_schedule():
+    """The checkpointing forward launch takes trajectories longest first (the last
+    call's step counts); each trajectory's integration, and so the gradient, is
+    the same bit for bit in any order."""
+    from menodax_b200 import autograd
+
+    cfg = systems.vdp_gradient_config(1, size=2048)
+    t_span = np.linspace(0.0, 100.0, 11)
+    w = np.random.default_rng(17).normal(size=(2048, len(t_span), 2))
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    autograd._capacity_hint.clear()
+    autograd._order_hint.clear()
+    ordered = _grads(rodas5P.solve, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], w, **kw)
+    assert len(autograd._order_hint) == 1
+    autograd._order_hint.clear()
+    plain = _grads(rodas5P.solve, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], w, **kw)
+    for a, b in zip(ordered, plain):
+        assert np.array_equal(a, b)

@@ -45,6 +45,7 @@ static inline float host_powf(float a, float b) { return std::pow(a, b); }
 #define __powf host_powf
 static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
 template <class T> static inline T __ldcg(const T* p) { return *p; }
+template <class T> static inline T __ldg(const T* p) { return *p; }
 """
 
 DRIVER = """

@@ -47,6 +47,14 @@ _capacity_hint: dict = {}
 # long integrations start in the persistent grid's first wave; results do not
 # depend on the order.
 _order_hint: dict = {}
+# Per problem key: the persistent grid fill of the checkpointing forward launch.
+# Ordered longest first, the long integrations want a lightly loaded device on
+# some systems (config 5's 2 states: 44 ms at half fill against 94 ms full) and a
+# full one on others (its 16-state ring: 0.47 s full against 1.36 s at half fill,
+# FP32 LUs), so the first two ordered calls time one fill each and later calls
+# keep the faster.
+FORWARD_FILLS = (0.5, 1.0)
+_fill_hint: dict = {}
 # The checkpoint layout of the most recent gradient forward pass (for reports).
 last_checkpoint: dict = {}
 
@@ -96,16 +104,28 @@ def _longest_first(accepted):
     return torch.argsort(accepted, descending=True, stable=True).to(torch.int32)
 
 
-def _half_fill(problem, n: int) -> int:
-    """Blocks of the forward passes' persistent launch: half the resident limit.
+def _forward_blocks(problem, n: int, fill: float = 0.5) -> int:
+    """Blocks of the forward passes' persistent launch: ``fill`` of the resident limit.
 
     Gradient ensembles are long stiff integrations with uneven step counts; the
     refill launch keeps lanes busy as trajectories finish, and at half the
     resident warps each runs with less contention (a 16-state ring's
-    checkpointing forward: 0.77 s against 1.21 s for the one-launch kernel;
-    unchanged for 2 states)."""
-    choice = autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 0.5, int(problem.options.team))
+    checkpointing forward in index order: 0.77 s against 1.21 s for the
+    one-launch kernel; unchanged for 2 states)."""
+    choice = autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, fill, int(problem.options.team))
     return autotune.grid_blocks(problem, choice, n)
+
+
+def _forward_fill(key, ordered: bool) -> float:
+    """The fill of this call's checkpointing forward launch: half when it runs
+    in index order, else the next untimed one of FORWARD_FILLS, then the faster."""
+    if not ordered:
+        return 0.5
+    timed = _fill_hint.setdefault(key, {})
+    for fill in FORWARD_FILLS:
+        if fill not in timed:
+            return fill
+    return min(timed, key=timed.get)
 
 
 # Trajectories per reverse launch (None: the whole ensemble in one launch).  The
@@ -180,7 +200,7 @@ class _EnsembleSolve(torch.autograd.Function):
             order = None
         if capacity is None:
             # First call for this problem: count the accepted steps with a plain solve.
-            _, counters = launch(problems["plain"], grid_blocks=_half_fill(problems["plain"], n), **kw)
+            _, counters = launch(problems["plain"], grid_blocks=_forward_blocks(problems["plain"], n), **kw)
             capacity = max(1, int(counters[0].max().item()) if n else 1)
             order = _longest_first(counters[0])
         while True:
@@ -193,9 +213,16 @@ class _EnsembleSolve(torch.autograd.Function):
             nbytes = problem.plan.checkpoint_size(n, capacity)
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
+            fill = _forward_fill(key, order is not None)
+            stream = torch.cuda.current_stream(y0.device)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity,
-                                    grid_blocks=_half_fill(problem, n), order=order, **kw)
+                                    grid_blocks=_forward_blocks(problem, n, fill), order=order, **kw)
+            e1.record(stream)
             needed = int(counters[0].max().item()) if n else 0
+            if order is not None and fill not in _fill_hint.get(key, {}):
+                _fill_hint.setdefault(key, {})[fill] = e0.elapsed_time(e1)
             if needed <= capacity:
                 break
             capacity = int(needed * 1.1) + 8

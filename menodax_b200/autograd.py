@@ -51,9 +51,10 @@ _order_hint: dict = {}
 # Ordered longest first, the long integrations want a lightly loaded device on
 # some systems (config 5's 2 states: 44 ms at half fill against 94 ms full) and a
 # full one on others (its 16-state ring: 0.47 s full against 1.36 s at half fill,
-# FP32 LUs), so the first two ordered calls time one fill each and later calls
-# keep the faster.
-FORWARD_FILLS = (0.5, 1.0)
+# FP32 LUs).  The first ordered call runs at half fill untimed (its launch also
+# loads the module); the next two time one fill each, and later calls keep the
+# faster.
+FORWARD_FILLS = (1.0, 0.5)
 _fill_hint: dict = {}
 # The checkpoint layout of the most recent gradient forward pass (for reports).
 last_checkpoint: dict = {}
@@ -116,16 +117,20 @@ def _forward_blocks(problem, n: int, fill: float = 0.5) -> int:
     return autotune.grid_blocks(problem, choice, n)
 
 
-def _forward_fill(key, ordered: bool) -> float:
-    """The fill of this call's checkpointing forward launch: half when it runs
-    in index order, else the next untimed one of FORWARD_FILLS, then the faster."""
+def _forward_fill(key, ordered: bool):
+    """``(fill, timed)`` for this call's checkpointing forward launch: half fill
+    when it runs in index order or is the first ordered call, then each of
+    FORWARD_FILLS once with its time recorded, then the faster."""
     if not ordered:
-        return 0.5
-    timed = _fill_hint.setdefault(key, {})
+        return 0.5, False
+    hint = _fill_hint.setdefault(key, {"warm": False, "times": {}})
+    if not hint["warm"]:
+        hint["warm"] = True
+        return 0.5, False
     for fill in FORWARD_FILLS:
-        if fill not in timed:
-            return fill
-    return min(timed, key=timed.get)
+        if fill not in hint["times"]:
+            return fill, True
+    return min(hint["times"], key=hint["times"].get), False
 
 
 # Trajectories per reverse launch (None: the whole ensemble in one launch).  The
@@ -213,7 +218,7 @@ class _EnsembleSolve(torch.autograd.Function):
             nbytes = problem.plan.checkpoint_size(n, capacity)
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
-            fill = _forward_fill(key, order is not None)
+            fill, trial = _forward_fill(key, order is not None)
             stream = torch.cuda.current_stream(y0.device)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -221,8 +226,8 @@ class _EnsembleSolve(torch.autograd.Function):
                                     grid_blocks=_forward_blocks(problem, n, fill), order=order, **kw)
             e1.record(stream)
             needed = int(counters[0].max().item()) if n else 0
-            if order is not None and fill not in _fill_hint.get(key, {}):
-                _fill_hint.setdefault(key, {})[fill] = e0.elapsed_time(e1)
+            if trial:
+                _fill_hint[key]["times"][fill] = e0.elapsed_time(e1)
             if needed <= capacity:
                 break
             capacity = int(needed * 1.1) + 8

@@ -234,7 +234,8 @@ class _EnsembleSolve(torch.autograd.Function):
             del ckpt
         _capacity_hint[key] = (max(needed + 8, int(needed * 1.1)), stride)
         _order_hint[key] = _longest_first(counters[0])
-        last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes)
+        last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes, forward_fill=fill,
+                               fill_times_ms=dict(_fill_hint.get(key, {}).get("times", {})))
         ctx.problem = problem
         ctx.capacity = capacity
         ctx.save_for_backward(pc, times, ckpt, ckpt_count)

@@ -56,6 +56,16 @@ _order_hint: dict = {}
 # faster.
 FORWARD_FILLS = (1.0, 0.5)
 _fill_hint: dict = {}
+# Problems remembered by the three hints above (oldest dropped first): the order
+# hint holds a device tensor per problem.
+HINT_PROBLEMS = 64
+
+
+def _remember(hints: dict, key, value) -> None:
+    hints.pop(key, None)
+    hints[key] = value
+    while len(hints) > HINT_PROBLEMS:
+        hints.pop(next(iter(hints)))
 # The checkpoint layout of the most recent gradient forward pass (for reports).
 last_checkpoint: dict = {}
 
@@ -123,7 +133,10 @@ def _forward_fill(key, ordered: bool):
     FORWARD_FILLS once with its time recorded, then the faster."""
     if not ordered:
         return 0.5, False
-    hint = _fill_hint.setdefault(key, {"warm": False, "times": {}})
+    hint = _fill_hint.get(key)
+    if hint is None:
+        hint = {"warm": False, "times": {}}
+        _remember(_fill_hint, key, hint)
     if not hint["warm"]:
         hint["warm"] = True
         return 0.5, False
@@ -232,8 +245,8 @@ class _EnsembleSolve(torch.autograd.Function):
                 break
             capacity = int(needed * 1.1) + 8
             del ckpt
-        _capacity_hint[key] = (max(needed + 8, int(needed * 1.1)), stride)
-        _order_hint[key] = _longest_first(counters[0])
+        _remember(_capacity_hint, key, (max(needed + 8, int(needed * 1.1)), stride))
+        _remember(_order_hint, key, _longest_first(counters[0]))
         last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes, forward_fill=fill,
                                fill_times_ms=dict(_fill_hint.get(key, {}).get("times", {})))
         ctx.problem = problem

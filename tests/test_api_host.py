@@ -96,3 +96,16 @@ def test_array_rhs_traces_into_the_primal_graph():
     assert src != plain and "mdx_rhs" in src
     with pytest.raises(ValueError, match="array_rhs must be a callable"):
         rodas5P.solve(systems.robertson, np.zeros(3), systems.ROBERTSON_TIMES, np.zeros(3), array_rhs=3)
+
+
+def test_gradient_hints_keep_a_bounded_number_of_problems():
+    from menodax_b200 import autograd
+
+    hints = {}
+    for k in range(autograd.HINT_PROBLEMS + 10):
+        autograd._remember(hints, ("problem", k), k)
+    assert len(hints) == autograd.HINT_PROBLEMS
+    assert ("problem", 0) not in hints and ("problem", autograd.HINT_PROBLEMS + 9) in hints
+    autograd._remember(hints, ("problem", 10), "again")   # refreshed: now the newest
+    autograd._remember(hints, ("problem", 999), 0)
+    assert ("problem", 10) in hints and ("problem", 11) not in hints

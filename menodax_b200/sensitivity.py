@@ -28,8 +28,14 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
+from menodax_b200 import _native, autotune
 from menodax_b200._ensemble import initial_step, launch, normalize_y0_params, pick_device, to_device
 from menodax_b200._problem import KernelOptions, get_problem
+
+# Per joint-solve problem: the trajectories of the last call, longest first (by
+# accepted steps), at most ORDER_HINT_PROBLEMS problems, oldest dropped first.
+ORDER_HINT_PROBLEMS = 64
+_order_hint: dict = {}
 
 
 @dataclass(frozen=True)
@@ -136,9 +142,24 @@ def solve(solver, ode_fn, y0, t_span, params, *, wrt_y0=True, wrt_params=True,
         times = t_span.detach().to(device=device, dtype=torch.float64).contiguous()
     else:
         times = torch.as_tensor(np.asarray(t_span, dtype=np.float64), device=device).contiguous()
+    # The persistent refill launch, trajectories longest first by the previous
+    # call's step counts for the same problem: the joint solves are long and
+    # uneven, and the order only moves when each trajectory runs (config 5's 2
+    # states: 324 ms plain, 207 ms persistent, 163 ms persistent longest first;
+    # the same gradients bit for bit).
+    key = (ode_fn, n_vars, n_params, options, n, tuple(times.tolist()), float(rtol), float(atol))
+    order = _order_hint.get(key)
+    if order is not None and (order.device != device or order.numel() != n):
+        order = None
+    choice = autotune.LaunchChoice(problem.plan.tpb, _native.MDX_LAUNCH_PERSISTENT, 1.0)
     hist, counters = launch(problem, y0=z0, times=times, params=to_device(p_t.detach(), device),
                             weights=None, dt0=initial_step(first_step), rtol=rtol, atol=atol,
-                            max_steps=max_steps, mode=0)
+                            max_steps=max_steps, mode=_native.MDX_LAUNCH_PERSISTENT,
+                            grid_blocks=autotune.grid_blocks(problem, choice, n), order=order)
+    _order_hint.pop(key, None)
+    _order_hint[key] = torch.argsort(counters[0], descending=True, stable=True).to(torch.int32)
+    while len(_order_hint) > ORDER_HINT_PROBLEMS:
+        _order_hint.pop(next(iter(_order_hint)))
     state, sens = split_augmented(hist, spec)
     if return_stats:
         from menodax_b200._ensemble import solver_stats

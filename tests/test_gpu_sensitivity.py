@@ -89,3 +89,18 @@ def test_jvp_contracts_the_sensitivities():
                                 wrt_y0=False, rtol=1e-8, atol=1e-12)
     expect = np.einsum("nsik,k->nsi", sens.cpu().numpy(), dp)
     np.testing.assert_allclose(tangent.cpu().numpy(), expect, rtol=1e-12, atol=1e-20)
+
+
+def test_joint_solve_visiting_order_changes_nothing():
+    """The joint solve's persistent launch takes trajectories longest first by the
+    previous call's step counts; the sensitivities are the same bit for bit as
+    in index order."""
+    cfg = systems.vdp_gradient_config(1, size=3000)
+    t_span = np.linspace(0.0, 100.0, 11)
+    kw = dict(rtol=cfg["rtol"], atol=cfg["atol"], lu_precision="fp64")
+    sensitivity._order_hint.clear()
+    first = sensitivity.solve("rodas5P", cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], **kw)
+    assert len(sensitivity._order_hint) == 1
+    ordered = sensitivity.solve("rodas5P", cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], **kw)
+    for a, b in zip(first, ordered):
+        assert torch.equal(a, b)

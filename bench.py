@@ -495,6 +495,7 @@ def measure_config(name, steps, warmup, rank, world, *, max_steps=100000, n_limi
 
     from menodax_b200 import _native, autotune
     from menodax_b200._ensemble import launch
+    from menodax_b200._frontend import longest_first
     from menodax_b200._problem import KernelOptions, get_problem
     from menodax_b200._sparsity import normalize_sparsity
     from workloads import systems
@@ -562,9 +563,14 @@ def measure_config(name, steps, warmup, rank, world, *, max_steps=100000, n_limi
         # kernel takes 25-36 ms on its first two launches).
         warm_start = time.perf_counter()
         done = 0
+        order = None
         while done < warmup or (time.perf_counter() - warm_start < WARM_S and done < WARM_MAX):
-            hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
+            hist, counters = launch(prob, mode=mode, grid_blocks=grid, order=order, **common)
             torch.cuda.synchronize()
+            if mode == _native.MDX_LAUNCH_PERSISTENT:
+                # As rodas5P.solve does from its second call on: the persistent
+                # launch takes the trajectories longest first by the last one's steps.
+                order = longest_first(counters[2])
             done += 1
         barrier(world)
         ms = []
@@ -574,7 +580,7 @@ def measure_config(name, steps, warmup, rank, world, *, max_steps=100000, n_limi
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            hist, counters = launch(prob, mode=mode, grid_blocks=grid, **common)
+            hist, counters = launch(prob, mode=mode, grid_blocks=grid, order=order, **common)
             e1.record(stream)
             ms.append((e0, e1))
         torch.cuda.nvtx.range_pop()

@@ -25,6 +25,30 @@ from menodax_b200._problem import KernelOptions, get_problem
 
 LAUNCH_MODES = ("auto", "plain", "persistent")
 
+# Per problem (the compiled options, ensemble size, save times, tolerances and
+# step cap): the trajectories of the last persistent launch, most attempted
+# steps first.  The next persistent launch of the same problem takes them in that
+# order, so the long integrations start in the grid's first wave instead of
+# setting the makespan from a late one (config 4's Brusselator 16.9 -> 15.0 ms,
+# the 32-state ring 7.5 -> 4.1 s); every trajectory's integration, and so the
+# result, is the same in any order.  At most ORDER_HINT_PROBLEMS problems are
+# remembered, oldest dropped first.
+ORDER_HINT_PROBLEMS = 64
+_order_hint: dict = {}
+
+
+def longest_first(loop_steps: torch.Tensor) -> torch.Tensor:
+    """The int32 visiting order of a persistent launch: trajectories by
+    descending attempted steps."""
+    return torch.argsort(loop_steps, descending=True, stable=True).to(torch.int32)
+
+
+def _remember_order(key, order) -> None:
+    _order_hint.pop(key, None)
+    _order_hint[key] = order
+    while len(_order_hint) > ORDER_HINT_PROBLEMS:
+        _order_hint.pop(next(iter(_order_hint)))
+
 
 def _is_torch(*xs):
     return any(isinstance(x, torch.Tensor) for x in xs)
@@ -108,8 +132,18 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
         # solve.  The persistent launch finishes one lane's row at a time, too
         # small a write for the host link, so its history is copied afterwards.
         streamed = mode == _native.MDX_LAUNCH_PLAIN
+    order = None
+    order_key = None
+    if mode == _native.MDX_LAUNCH_PERSISTENT:
+        order_key = (ode_fn, n_vars, n_params, options, n, tuple(times.tolist()), float(rtol), float(atol),
+                     int(max_steps), int(grid_blocks))
+        order = _order_hint.get(order_key)
+        if order is not None and (order.device != device or order.numel() != n):
+            order = None
     hist, counters = launch(problem, mode=mode, grid_blocks=grid_blocks, hook_out=hook_out,
-                            hist_host=hist_h if streamed else None, **common)
+                            hist_host=hist_h if streamed else None, order=order, **common)
+    if order_key is not None and n > 0:
+        _remember_order(order_key, longest_first(counters[2]))
     if hist_h is None:
         result = (hist,) if hook_out is None else (hist, hook_out)
         if return_stats:

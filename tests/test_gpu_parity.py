@@ -224,3 +224,21 @@ def test_array_rhs_evaluates_the_stages():
     same = (np.asarray(s1["loop_steps"]) == np.asarray(s2["loop_steps"]))
     assert same.mean() >= 0.999
     np.testing.assert_allclose(h2[same], h1[same], rtol=1e-9, atol=1e-15)
+
+
+def test_persistent_solve_visiting_order_changes_nothing():
+    """From its second call on a persistent solve takes the trajectories longest
+    first by the previous call's attempted steps; the results are the same bit
+    for bit."""
+    from menodax_b200 import _frontend
+
+    cfg = systems.vdp_ring_config(4, size=2000)
+    t_span = np.linspace(0.0, 30.0, 20)
+    kw = dict(rtol=1e-6, atol=1e-8, sparsity=cfg["sparsity"], launch="persistent", return_stats=True)
+    _frontend._order_hint.clear()
+    h1, s1 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], **kw)
+    assert len(_frontend._order_hint) == 1
+    h2, s2 = rodas5P.solve(cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], **kw)
+    assert np.array_equal(h1, h2)
+    for k in ("accepted_steps", "rejected_steps", "loop_steps"):
+        assert np.array_equal(np.asarray(s1[k]), np.asarray(s2[k]))

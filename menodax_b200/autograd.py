@@ -47,17 +47,19 @@ _capacity_hint: dict = {}
 # long integrations start in the persistent grid's first wave; results do not
 # depend on the order.
 _order_hint: dict = {}
-# Per problem key: the persistent grid fill of the checkpointing forward launch.
-# Ordered longest first, the long integrations want a lightly loaded device on
-# some systems (config 5's 2 states: 44 ms at half fill against 94 ms full) and a
-# full one on others (its 16-state ring: 0.47 s full against 1.36 s at half fill,
-# FP32 LUs).  The first ordered call runs at half fill untimed (its launch also
-# loads the module); the next two time one fill each, and later calls keep the
-# faster.
-FORWARD_FILLS = (1.0, 0.5)
-_fill_hint: dict = {}
-# Problems remembered by the three hints above (oldest dropped first): the order
-# hint holds a device tensor per problem.
+# The persistent grid fill of the checkpointing forward launch once it takes
+# trajectories longest first.  Measured on config 5 (B200): the 2-state system
+# wants a lightly loaded device (FP64 42 ms at half fill against 59-60 ms full,
+# FP32 LUs 37-41 against 45-51 ms), the 16-state ring a full one (FP64 0.57 s
+# full against 0.76 s at half fill, FP32 LUs 0.47 against 1.36 s): a small
+# system's long integrations run fastest with few neighbours on their SM, a
+# large one's spilled steps need the full grid's warps to hide their memory
+# latency.
+FORWARD_FILL_SMALL = 0.5
+FORWARD_FILL_LARGE = 1.0
+FORWARD_FILL_SMALL_VARS = 8
+# Problems remembered by the hints above (oldest dropped first): the order hint
+# holds a device tensor per problem.
 HINT_PROBLEMS = 64
 
 
@@ -66,6 +68,8 @@ def _remember(hints: dict, key, value) -> None:
     hints[key] = value
     while len(hints) > HINT_PROBLEMS:
         hints.pop(next(iter(hints)))
+
+
 # The checkpoint layout of the most recent gradient forward pass (for reports).
 last_checkpoint: dict = {}
 
@@ -127,23 +131,12 @@ def _forward_blocks(problem, n: int, fill: float = 0.5) -> int:
     return autotune.grid_blocks(problem, choice, n)
 
 
-def _forward_fill(key, ordered: bool):
-    """``(fill, timed)`` for this call's checkpointing forward launch: half fill
-    when it runs in index order or is the first ordered call, then each of
-    FORWARD_FILLS once with its time recorded, then the faster."""
-    if not ordered:
-        return 0.5, False
-    hint = _fill_hint.get(key)
-    if hint is None:
-        hint = {"warm": False, "times": {}}
-        _remember(_fill_hint, key, hint)
-    if not hint["warm"]:
-        hint["warm"] = True
-        return 0.5, False
-    for fill in FORWARD_FILLS:
-        if fill not in hint["times"]:
-            return fill, True
-    return min(hint["times"], key=hint["times"].get), False
+def _forward_fill(n_vars: int, ordered: bool) -> float:
+    """The fill of a checkpointing forward launch: half in index order, else by
+    the system's size once the long trajectories go first."""
+    if not ordered or n_vars <= FORWARD_FILL_SMALL_VARS:
+        return FORWARD_FILL_SMALL
+    return FORWARD_FILL_LARGE
 
 
 # Trajectories per reverse launch (None: the whole ensemble in one launch).  The
@@ -231,24 +224,17 @@ class _EnsembleSolve(torch.autograd.Function):
             nbytes = problem.plan.checkpoint_size(n, capacity)
             ckpt = torch.empty(max(1, nbytes // 8), dtype=torch.float64, device=y0.device)
             ckpt_count = torch.empty(n, dtype=torch.int32, device=y0.device)
-            fill, trial = _forward_fill(key, order is not None)
-            stream = torch.cuda.current_stream(y0.device)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+            fill = _forward_fill(problems["plain"].n_vars, order is not None)
             hist, counters = launch(problem, ckpt=ckpt, ckpt_count=ckpt_count, ckpt_capacity=capacity,
                                     grid_blocks=_forward_blocks(problem, n, fill), order=order, **kw)
-            e1.record(stream)
             needed = int(counters[0].max().item()) if n else 0
-            if trial:
-                _fill_hint[key]["times"][fill] = e0.elapsed_time(e1)
             if needed <= capacity:
                 break
             capacity = int(needed * 1.1) + 8
             del ckpt
         _remember(_capacity_hint, key, (max(needed + 8, int(needed * 1.1)), stride))
         _remember(_order_hint, key, _longest_first(counters[0]))
-        last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes, forward_fill=fill,
-                               fill_times_ms=dict(_fill_hint.get(key, {}).get("times", {})))
+        last_checkpoint.update(stride=stride, capacity=capacity, bytes=nbytes, forward_fill=fill)
         ctx.problem = problem
         ctx.capacity = capacity
         ctx.save_for_backward(pc, times, ckpt, ckpt_count)

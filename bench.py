@@ -287,7 +287,7 @@ def gradient_errors(cfg, target, grads, sample):
 
 # --------------------------------------------------------------------------- gradients
 def measure_gradients(n, steps, warmup, rank, world, n_osc=1, oracle_checks=False, ring_forward_sens=False):
-    """Config 5: discrete-adjoint value_and_grad of sum((y - target)^2), device-timed.
+    """Stiff Van der Pol gradients: discrete-adjoint value_and_grad of sum((y - target)^2), device-timed.
 
     VdP (n_osc=1: 2 states), mu ~ log-uniform[10, 500], y0 and mu differentiated,
     20 saves on [0, 1000], rtol 1e-6, atol 1e-8, FP64; targets are the same solve

@@ -29,10 +29,11 @@ LAUNCH_MODES = ("auto", "plain", "persistent")
 # step cap): the trajectories of the last persistent launch, most attempted
 # steps first.  The next persistent launch of the same problem takes them in that
 # order, so the long integrations start in the grid's first wave instead of
-# setting the makespan from a late one (config 4's Brusselator 16.9 -> 15.0 ms,
-# the 32-state ring 7.5 -> 4.1 s); every trajectory's integration, and so the
-# result, is the same in any order.  At most ORDER_HINT_PROBLEMS problems are
-# remembered, oldest dropped first.
+# setting the makespan from a late one (the 64-state Brusselator's 16,384
+# trajectories 16.9 -> 15.0 ms, the 32-state Van der Pol ring's 32,768 7.5 ->
+# 4.1 s); every trajectory's integration, and so the result, is the same in any
+# order.  At most ORDER_HINT_PROBLEMS problems are remembered, oldest dropped
+# first.
 ORDER_HINT_PROBLEMS = 64
 _order_hint: dict = {}
 

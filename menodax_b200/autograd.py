@@ -48,8 +48,9 @@ _capacity_hint: dict = {}
 # depend on the order.
 _order_hint: dict = {}
 # The persistent grid fill of the checkpointing forward launch once it takes
-# trajectories longest first.  Measured on config 5 (B200): the 2-state system
-# wants a lightly loaded device (FP64 42 ms at half fill against 59-60 ms full,
+# trajectories longest first.  Measured on the stiff Van der Pol gradient
+# ensembles (65,536 trajectories, B200): the 2-state system wants a lightly
+# loaded device (FP64 42 ms at half fill against 59-60 ms full,
 # FP32 LUs 37-41 against 45-51 ms), the 16-state ring a full one (FP64 0.57 s
 # full against 0.76 s at half fill, FP32 LUs 0.47 against 1.36 s): a small
 # system's long integrations run fastest with few neighbours on their SM, a
@@ -154,9 +155,10 @@ def reverse_chunk(problem, n: int) -> int:
 # number of checkpoint segments is cut into chunks of at most that many, reversed
 # in parallel and composed (None: never, the default).  A chunk costs n_vars + 1
 # sweeps (its transfer matrix's columns and its offset), so splitting pays only
-# when a few trajectories are far longer than the rest; on config 5's ensembles
-# the long trajectories are a sizeable fraction (at 2.5 x the mean, 5,141 of
-# 65,536 2-state trajectories), and splitting them made the reverse pass slower.
+# when a few trajectories are far longer than the rest; on the stiff Van der Pol
+# gradient ensembles the long trajectories are a sizeable fraction (at 2.5 x the
+# mean, 5,141 of 65,536 2-state trajectories), and splitting them made the
+# reverse pass slower.
 REVERSE_SPLIT: float | None = None
 
 

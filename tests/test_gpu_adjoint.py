@@ -192,7 +192,7 @@ def test_sparse_lu_adjoint_matches_dense(lu_precision):
 
 @pytest.mark.parametrize("n_osc", [1, 3])
 def test_vdp_gradient_config_matches_oracle_forward_sensitivities(oracle, n_osc):
-    """Config 5's system and loss: sum((y - target)^2) over the saves, targets
+    """The stiff Van der Pol gradient workload's system and loss: sum((y - target)^2) over the saves, targets
     from mu * 1.05, y0 and mu differentiated.  The discrete adjoint of the solve
     equals the oracle's forward sensitivities on the same step sequence (the
     reference's sens_error_control=False), within 1e-5 relative."""
@@ -215,7 +215,7 @@ def test_vdp_gradient_config_matches_oracle_forward_sensitivities(oracle, n_osc)
 
 def test_fp32_lu_adjoint_agrees_with_fp64_on_a_short_horizon():
     """The FP32-LU adjoint (fast arithmetic) differentiates its own, slightly
-    different solution; over a few relaxation cycles of config 5's system the two
+    different solution; over a few relaxation cycles of the 2-state stiff Van der Pol system the two
     gradients agree to 1e-4 (median) -- over t in [0, 1000] the loss amplifies the
     rtol-level solution differences into gradient differences of several percent,
     for any two solves that take different steps."""

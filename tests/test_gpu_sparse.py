@@ -82,7 +82,7 @@ def test_brusselator_64_fp32_sparse_as_accurate_as_fp64(oracle):
 
 
 def test_vdp_ring_fp32_sparse_as_accurate_as_fp64(oracle):
-    """Config 3's product path (FP32 LU, fast arithmetic, AMD-ordered sparse LU)
+    """The Van der Pol ring's product path (FP32 LU, fast arithmetic, AMD-ordered sparse LU)
     against a tight FP64 oracle, by the distribution of each trajectory's worst
     relative error: median and 90th percentile as small as the FP64-LU solve's at
     the same tolerance (to 1.5x + 10 rtol), the worst trajectory within 3x.  The

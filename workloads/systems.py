@@ -57,7 +57,7 @@ def lorenz_divergence_scenario(size: int, seed: int = 42, divergence: float = 1.
 
 
 def lorenz_config(size: int = 4096, seed: int = 42):
-    """Config 1: sigma=10, beta=8/3, rho ~ U[0, 28), y0 = (1, 0, 0), t in [0, 1], 10 saves."""
+    """Lorenz ensemble: sigma=10, beta=8/3, rho ~ U[0, 28), y0 = (1, 0, 0), t in [0, 1], 10 saves."""
     rng = np.random.default_rng(seed)
     params = rng.uniform(0.0, 28.0, size=(size, 1))
     y0 = np.broadcast_to(np.array([1.0, 0.0, 0.0]), (size, 3)).copy()
@@ -81,7 +81,7 @@ ROBERTSON_PARAMS = np.array([0.04, 1e4, 3e7])
 
 
 def robertson_config(size: int = 65536, seed: int = 42):
-    """Config 2: k1=0.04, k2=3e7, k3=1e4 each x log-uniform[0.5, 2]; y0=(1,0,0);
+    """Robertson kinetics ensemble: k1=0.04, k2=3e7, k3=1e4 each x log-uniform[0.5, 2]; y0=(1,0,0);
     20 save times on [0, 1e5] (0 then 19 log-spaced from 1e-5); rtol 1e-6, atol 1e-10.
 
     The rates are mapped onto the module's ``[k1, k3, k2]`` column order."""
@@ -135,7 +135,7 @@ def vdp_sparsity(n_osc: int, coupling_range: int = 1) -> np.ndarray:
 
 
 def vdp_ring_config(n_osc: int, size: int = 32768, seed: int = 42):
-    """Config 3: mu ~ log-uniform[10, 1000] as p0, epsilon = 0.1 coupling, omega = 1,
+    """Stiff Van der Pol ring ensemble: mu ~ log-uniform[10, 1000] as p0, epsilon = 0.1 coupling, omega = 1,
     y0 = (2, 0) + N(0, 0.1) per oscillator, t in [0, 3000], 50 saves, rtol 1e-6, atol 1e-8."""
     ode_fn, base = make_vdp_system(n_osc, mu=1.0, d=0.1, omega=1.0)
     rng = np.random.default_rng(seed)
@@ -177,7 +177,7 @@ def brusselator_pattern(n_grid: int) -> np.ndarray:
 
 
 def brusselator_config(n_grid: int = 32, size: int = 16384, seed: int = 42):
-    """Config 4: 32 points (64 states), alpha = 1/50, A = 1, B ~ U[2.5, 3.5], periodic;
+    """Brusselator ensemble: 32 points (64 states), alpha = 1/50, A = 1, B ~ U[2.5, 3.5], periodic;
     u = 1 + sin(2 pi x) + N(0, 0.01), v = 3; t in [0, 10], 10 saves; rtol 1e-6, atol 1e-8."""
     rng = np.random.default_rng(seed)
     b = rng.uniform(2.5, 3.5, size=(size, 1))
@@ -191,7 +191,7 @@ def brusselator_config(n_grid: int = 32, size: int = 16384, seed: int = 42):
 
 # --- Van der Pol adjoint problem ----------------------------------------------------
 def vdp_gradient_config(n_osc: int, size: int = 65536, seed: int = 42):
-    """Config 5: mu ~ log-uniform[10, 500]; differentiate y0 and mu; 20 saves on [0, 1000];
+    """Stiff Van der Pol gradient ensemble: mu ~ log-uniform[10, 500]; differentiate y0 and mu; 20 saves on [0, 1000];
     targets from mu x 1.05 (computed by the caller); rtol 1e-6, atol 1e-8, FP64."""
     ode_fn, base = make_vdp_system(n_osc, mu=1.0, d=0.1, omega=1.0)
     rng = np.random.default_rng(seed)

@@ -34,7 +34,7 @@ LAUNCH_MODES = ("auto", "plain", "persistent")
 # 4.1 s); every trajectory's integration, and so the result, is the same in any
 # order.  At most ORDER_HINT_PROBLEMS problems are remembered, oldest dropped
 # first.
-ORDER_HINT_PROBLEMS = 64
+ORDER_HINT_PROBLEMS = 16
 _order_hint: dict = {}
 
 

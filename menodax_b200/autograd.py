@@ -61,7 +61,7 @@ FORWARD_FILL_LARGE = 1.0
 FORWARD_FILL_SMALL_VARS = 8
 # Problems remembered by the hints above (oldest dropped first): the order hint
 # holds a device tensor per problem.
-HINT_PROBLEMS = 64
+HINT_PROBLEMS = 16
 
 
 def _remember(hints: dict, key, value) -> None:

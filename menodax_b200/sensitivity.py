@@ -34,7 +34,7 @@ from menodax_b200._problem import KernelOptions, get_problem
 
 # Per joint-solve problem: the trajectories of the last call, longest first (by
 # accepted steps), at most ORDER_HINT_PROBLEMS problems, oldest dropped first.
-ORDER_HINT_PROBLEMS = 64
+ORDER_HINT_PROBLEMS = 16
 _order_hint: dict = {}
 
 

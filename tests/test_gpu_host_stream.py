@@ -62,6 +62,19 @@ def test_tsit5_host_copy(launch_mode):
     _assert_same(host, on_dev)
 
 
+@pytest.mark.parametrize("max_steps", [100000, 40])
+def test_chunked_host_copy_many_saves(max_steps):
+    """200 save times (a 4,800-byte row per trajectory) and a ragged last warp;
+    with a step cap, capped trajectories' later rows hold the frozen state
+    written when they stop."""
+    cfg = systems.robertson_config(size=1000)
+    t_span = np.concatenate([[0.0], np.logspace(-5, 5, 199)])
+    host, on_dev = _both(rodas5P, cfg["ode_fn"], cfg["y0"], t_span, cfg["params"], rtol=cfg["rtol"],
+                         atol=cfg["atol"], lu_precision="fp32", launch="plain", max_steps=max_steps)
+    assert host.shape == (1000, 200, 3)
+    _assert_same(host, on_dev)
+
+
 def _sum_first_component(save_idx, y, t, p, acc):
     acc[0] += y[0]
 

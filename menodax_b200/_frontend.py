@@ -22,6 +22,7 @@ from menodax_b200._ensemble import (
     to_device,
 )
 from menodax_b200._problem import KernelOptions, get_problem
+from menodax_b200.autotune import longest_first
 
 LAUNCH_MODES = ("auto", "plain", "persistent")
 
@@ -36,12 +37,6 @@ LAUNCH_MODES = ("auto", "plain", "persistent")
 # first.
 ORDER_HINT_PROBLEMS = 16
 _order_hint: dict = {}
-
-
-def longest_first(loop_steps: torch.Tensor) -> torch.Tensor:
-    """The int32 visiting order of a persistent launch: trajectories by
-    descending attempted steps."""
-    return torch.argsort(loop_steps, descending=True, stable=True).to(torch.int32)
 
 
 def _remember_order(key, order) -> None:
@@ -104,6 +99,8 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
     hook_out = None
     if options.save_hook is not None:
         hook_out = torch.empty((n, options.hook_size), dtype=torch.float64, device=device)
+    input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
+    host_results = not (torch_io and input_on_gpu)
     if launch_mode == "auto" and n >= AUTOTUNE_MIN_TRAJECTORIES and hook_out is None:
         from menodax_b200 import autotune
 
@@ -113,6 +110,9 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
         problem = get_problem(ode_fn, n_vars, n_params, options)
         mode = choice.mode
         grid_blocks = autotune.grid_blocks(problem, choice, n)
+        if host_results and autotune.streams_to_host(choice):
+            mode = _native.MDX_LAUNCH_PLAIN
+            grid_blocks = 0
     else:
         problem = get_problem(ode_fn, n_vars, n_params, options)
     n_save = int(t_d.shape[0])
@@ -122,10 +122,9 @@ def run(ode_fn, y0, t_span, params, options: KernelOptions, *, rtol, atol, first
                 f"the save hook reads or writes {name} at save_idx + {hi if lo >= 0 else lo}, "
                 f"outside its {length} entries for {n_save} save times"
             )
-    input_on_gpu = any(isinstance(x, torch.Tensor) and x.is_cuda for x in (y0, params))
     hist_h = None
     streamed = False
-    if not (torch_io and input_on_gpu):
+    if host_results:
         hist_h = torch.empty((n, n_save if options.save_history else 1, problem.n_system),
                              dtype=torch.float64, pin_memory=True)
         # Host results of a one-launch solve: each warp (or team) writes its

@@ -130,11 +130,28 @@ def grid_blocks(problem, choice: LaunchChoice, n: int) -> int:
     return max(1, int(min(full, needed) * choice.grid_fill))
 
 
+def streams_to_host(choice: LaunchChoice) -> bool:
+    """Whether a solve whose results go to host memory should run the one-launch
+    kernel of ``choice``'s module instead of ``choice`` itself.  A fully filled
+    persistent thread launch is picked only for short integrations (every
+    trajectory finished within the probe's step cap), where the history's trip
+    across the host link takes longer than the kernel; the one-launch kernel's
+    warps copy their rows to the host as they finish, which the persistent
+    launch cannot do in whole rows, so it gets the history there sooner."""
+    return choice.mode == _native.MDX_LAUNCH_PERSISTENT and choice.team == 0 and choice.grid_fill == 1.0
+
+
+def longest_first(loop_steps: torch.Tensor) -> torch.Tensor:
+    """The int32 visiting order of a persistent launch: trajectories by
+    descending attempted steps (stable, so ties keep index order)."""
+    return torch.argsort(loop_steps, descending=True, stable=True).to(torch.int32)
+
+
 def _timed_launch(problem, choice, stream, *, n, y0, times, params, weights, dt0, rtol, atol, max_steps,
-                  n_save_hist):
+                  n_save_hist, order=None):
     kw = dict(y0=y0[:n], times=times, params=params[:n], weights=weights[:n] if weights is not None else None,
               dt0=dt0, rtol=rtol, atol=atol, max_steps=max_steps, mode=choice.mode, n_save_hist=n_save_hist,
-              grid_blocks=grid_blocks(problem, choice, n))
+              grid_blocks=grid_blocks(problem, choice, n), order=order)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -238,11 +255,16 @@ def tune(ode_fn, n_vars, n_params, options, *, y0, times, params, weights, dt0, 
     # for the probe set and a full-device ensemble, so it bounds one candidate.
     launches = 2 * len(buildable)
     sample = n if probe_s * launches <= BUDGET_S else m
+    # Persistent candidates are timed as the front end runs them once a problem
+    # has been solved: longest first by the probe's step counts, so each warp
+    # takes trajectories of about the same length.
+    order = longest_first(counters[2][:sample])
     best = None
     for choice in buildable:
         prob = problem_for(choice)
-        _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, **inputs)
-        secs, _ = _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, **inputs)
+        visit = order if choice.mode == _native.MDX_LAUNCH_PERSISTENT else None
+        _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, order=visit, **inputs)
+        secs, _ = _timed_launch(prob, choice, stream, n=sample, max_steps=max_steps, order=visit, **inputs)
         if best is None or secs < best[0]:
             best = (secs, choice)
     with _lock:

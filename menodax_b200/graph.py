@@ -57,6 +57,7 @@ class GraphedSolve:
         self._options = options
         self._launch_mode = launch_mode
         self._graph = None
+        self._order = None
         self._stream = torch.cuda.Stream(device=dev)
 
     def _capture(self):
@@ -75,6 +76,12 @@ class GraphedSolve:
         with torch.cuda.stream(self._stream):
             launch(problem, **kw)  # loads the module and sizes the workspace before capture
             self._stream.synchronize()
+            if choice.mode == _native.MDX_LAUNCH_PERSISTENT:
+                # The captured persistent launch visits the trajectories longest
+                # first by this first solve's step counts (any order gives the
+                # same results; similar lengths in a warp finish together).
+                self._order = autotune.longest_first(self.counters[2])
+                kw["order"] = self._order
             graph = torch.cuda.CUDAGraph()
             with torch.cuda.graph(graph, stream=self._stream):
                 launch(problem, **kw)

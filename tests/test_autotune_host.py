@@ -160,3 +160,36 @@ def test_fp64_stage_solves_are_a_candidate_for_mid_sized_thread_kernels(fake_dev
         rec = Recorder(lambda c, m, s: 1.0, steps=10)
         _tune(fn, n, opts, rec, monkeypatch)
         assert {c.wide_solve for c, _, _ in rec.calls} == {None}
+
+
+def test_persistent_candidates_are_timed_longest_first(fake_device, monkeypatch):
+    """Short integrations: every persistent candidate is timed visiting the
+    trajectories longest first by the probe's step counts (as the front end runs
+    a problem from its second solve on); plain candidates take index order."""
+    fn, n, pattern = _ring(4)
+    opts = KernelOptions(lu_precision="fp32", fast=True, sparsity=pattern)
+    seen = []
+
+    def timed(problem, choice, stream, *, n, max_steps, order=None, **_):
+        seen.append((choice, n, max_steps, order))
+        counters = torch.zeros((4, n), dtype=torch.int32)
+        counters[2] = (torch.arange(n, dtype=torch.int32) * 7) % 13 + 100
+        return 0.010 if choice.mode == PERSISTENT and choice.grid_fill == 1.0 else 0.020, counters
+
+    choice = _tune(fn, n, opts, timed, monkeypatch, n=256)
+    assert (choice.mode, choice.grid_fill, choice.team) == (PERSISTENT, 1.0, 0)
+    steps = (torch.arange(256, dtype=torch.int32) * 7) % 13 + 100
+    expected = torch.argsort(steps, descending=True, stable=True).to(torch.int32)
+    full = [(c, o) for c, _, s, o in seen if s == 100000]
+    assert full and all((o is None) == (c.mode == PLAIN) for c, o in full)
+    for c, o in full:
+        if o is not None:
+            assert o.dtype == torch.int32 and torch.equal(o, expected)
+    assert torch.equal(autotune.longest_first(steps), expected)
+
+
+def test_host_results_of_short_persistent_thread_launches_stream_from_the_one_launch_kernel():
+    assert autotune.streams_to_host(autotune.LaunchChoice(128, PERSISTENT, 1.0, 0))
+    assert not autotune.streams_to_host(autotune.LaunchChoice(128, PERSISTENT, 0.5, 0))
+    assert not autotune.streams_to_host(autotune.LaunchChoice(128, PERSISTENT, 1.0, 8))
+    assert not autotune.streams_to_host(autotune.LaunchChoice(128, PLAIN, 0.0, 0))

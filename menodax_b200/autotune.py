@@ -26,7 +26,10 @@ candidates beside the register ones.
 Tuning is bounded in time.  The first candidate runs on the whole ensemble
 with at most ``PROBE_STEPS`` steps per trajectory.  When that finishes every
 trajectory, its time is a launch's, and the candidates are timed in full, or on
-the leading ``PROBE`` trajectories when that would exceed ``BUDGET_S``.  When it
+the leading ``PROBE`` trajectories when that would exceed ``BUDGET_S``; the
+persistent ones visit the trajectories longest first by the probe's step
+counts, as the front end runs them once it has solved the problem before (a
+warp of trajectories of about the same length finishes together).  When it
 hits the step cap the integrations are long (tens of thousands of steps): the
 plain candidates are ranked by the same capped run, which measures the cost of
 a step with the ensemble resident, and the winner runs as a persistent refill
